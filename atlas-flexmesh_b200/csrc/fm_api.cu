@@ -1,0 +1,1014 @@
+// fm_api.cu — the C ABI (include/fm_api.h) over the FlexMesh kernels.
+//
+// The context owns the mesh structures, the CSR pattern, the stiffness and
+// factor buffers and the solver work vectors on one device and stream.
+// Host-side loops (PCG iterations, Newton iterations, load steps) launch
+// kernels and read back only scalars (norms, stop flags).
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "fm_api.h"
+#include "fm_kernels.hpp"
+#include "fm_setup.hpp"
+
+namespace {
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    // (re)allocate to at least count elements; contents undefined
+    cudaError_t reserve(size_t count) {
+        if (count <= n && p) return cudaSuccess;
+        release();
+        if (count == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return e;
+        }
+        n = count;
+        return cudaSuccess;
+    }
+};
+
+struct SolverCsr {
+    uint32_t n = 0;
+    uint64_t nnz = 0;
+    uint32_t max_row = 0;
+    DevBuf<uint32_t> rp, ci, dpos, upos, fwd, bwd;
+    std::vector<uint32_t> h_rp, h_ci;
+    fm::CsrDev view() const {
+        fm::CsrDev v;
+        v.n = n;
+        v.rp = rp.p;
+        v.ci = ci.p;
+        v.dpos = dpos.p;
+        v.upos = upos.p;
+        v.fwd_order = fwd.p;
+        v.bwd_order = bwd.p;
+        v.max_row = max_row;
+        return v;
+    }
+};
+
+template <typename T>
+struct Work {
+    DevBuf<T> K, LU, diag, r, z, p, Ap, t, b, x;
+    bool factor_valid = false;
+};
+
+}  // namespace
+
+struct fm_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+
+    // mesh
+    uint32_t nn = 0, ne = 0, n = 0;
+    uint64_t nnz = 0;
+    std::vector<double> h_xyz;
+    std::vector<uint32_t> h_conn;
+    std::vector<uint8_t> h_skip;
+    fm::NodeGraph graph;
+    fm::Incidence inc;
+    DevBuf<double> xyz;
+    DevBuf<uint4> conn;
+    DevBuf<uint32_t> nbr_ptr, nbr, inc_ptr, inc_e;
+    SolverCsr fem;   // solve pattern of the mesh
+    SolverCsr gen;   // generic CSR (fm_csr_pcg_ilu0)
+    std::vector<uint32_t> lvl_fwd_ptr, lvl_fwd_rows, lvl_bwd_ptr, lvl_bwd_rows;
+
+    // material
+    bool has_mat = false;
+    int mat_mode = 0;
+    double nu = 0.3, mu_s = 0, lam_s = 0, c_mu = 0, c_lam = 0, inv_cnu = 0;
+    DevBuf<double> m0, m1;
+
+    // boundary conditions
+    bool has_bc = false, has_bcval = false;
+    DevBuf<uint8_t> mask;
+    DevBuf<double> bcval;
+
+    // reference-pattern assembly
+    DevBuf<int32_t> ref_slot;
+    DevBuf<double> ke_scratch;
+
+    // solver state
+    Work<double> w64;
+    Work<float> w32;
+    DevBuf<double> gen_K, gen_LU, gen_diag;
+    DevBuf<unsigned> done;
+    unsigned epoch = 0;
+    DevBuf<fm::DevScalars> sc;
+    fm::DevScalars* h_sc = nullptr;  // pinned mirror
+    DevBuf<double> partials;
+    DevBuf<double> vec_a, vec_b, vec_c;  // FP64 scratch (Newton R, du, trial u)
+    int grid_trsv64 = 0, grid_trsv32 = 0;
+
+    unsigned* status() { return &sc.p->status; }
+    unsigned* counter() { return &sc.p->counter[0]; }
+};
+
+namespace {
+
+fm_status fail(fm_ctx* c, fm_status st, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return st;
+}
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(c, e_ == cudaErrorMemoryAllocation ? FM_ERR_OOM : FM_ERR_CUDA,     \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+#define TRY(expr)                       \
+    do {                                \
+        fm_status s_ = (expr);          \
+        if (s_ != FM_OK) return s_;     \
+    } while (0)
+
+template <typename T>
+cudaError_t upload(DevBuf<T>& d, const T* h, size_t count, cudaStream_t s) {
+    cudaError_t e = d.reserve(count ? count : 1);
+    if (e != cudaSuccess) return e;
+    if (count) e = cudaMemcpyAsync(d.p, h, count * sizeof(T), cudaMemcpyHostToDevice, s);
+    return e;
+}
+
+fm_status device_flags(fm_ctx* c, uint32_t* flags) {
+    CK(cudaMemcpyAsync(c->h_sc, c->sc.p, sizeof(fm::DevScalars), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *flags = c->h_sc->status;
+    return FM_OK;
+}
+
+// Translate fatal device flags into a status
+fm_status check_flags(fm_ctx* c, uint32_t flags, const char* where) {
+    if (flags & FM_FLAG_TIMEOUT)
+        return fail(c, FM_ERR_TIMEOUT, "%s: a bounded dependency wait expired", where);
+    if (flags & FM_FLAG_NONFINITE)
+        return fail(c, FM_ERR_NONFINITE, "%s: non-finite value produced", where);
+    return FM_OK;
+}
+
+fm_status sync_scalars(fm_ctx* c) {
+    CK(cudaMemcpyAsync(c->h_sc, c->sc.p, sizeof(fm::DevScalars), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FM_OK;
+}
+
+fm::MeshDev mesh_view(const fm_ctx* c) {
+    fm::MeshDev m;
+    m.n_nodes = c->nn;
+    m.n_elems = c->ne;
+    m.xyz = c->xyz.p;
+    m.conn = c->conn.p;
+    m.nbr_ptr = c->nbr_ptr.p;
+    m.nbr = c->nbr.p;
+    m.inc_ptr = c->inc_ptr.p;
+    m.inc = c->inc_e.p;
+    m.mask = c->has_bc ? c->mask.p : nullptr;
+    m.mat_mode = c->mat_mode;
+    m.m0 = c->m0.p;
+    m.m1 = c->m1.p;
+    m.mu_s = c->mu_s;
+    m.lam_s = c->lam_s;
+    m.c_mu = c->c_mu;
+    m.c_lam = c->c_lam;
+    m.inv_cnu = c->inv_cnu;
+    return m;
+}
+
+// Build the solver CSR (ascending columns) on host and upload: row
+// pointers, columns, first-diagonal/first-upper positions and the DOF-level
+// dependency orders that the sync-free kernels walk.
+fm_status setup_solver_csr(fm_ctx* c, SolverCsr& S, uint32_t n, std::vector<uint32_t>&& rp,
+                           std::vector<uint32_t>&& ci, bool keep_levels) {
+    S.n = n;
+    S.nnz = rp[n];
+    std::vector<uint32_t> dpos(n), upos(n);
+    uint32_t max_row = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t k = rp[i];
+        while (k < rp[i + 1] && ci[k] < i) ++k;
+        dpos[i] = k;
+        while (k < rp[i + 1] && ci[k] <= i) ++k;
+        upos[i] = k;
+        max_row = std::max(max_row, rp[i + 1] - rp[i]);
+    }
+    S.max_row = max_row;
+    std::vector<uint32_t> fp, fr, bp, br;
+    fm::csr_levels(n, rp.data(), ci.data(), true, fp, fr);
+    fm::csr_levels(n, rp.data(), ci.data(), false, bp, br);
+    CK(upload(S.rp, rp.data(), rp.size(), c->stream));
+    CK(upload(S.ci, ci.data(), ci.size(), c->stream));
+    CK(upload(S.dpos, dpos.data(), n, c->stream));
+    CK(upload(S.upos, upos.data(), n, c->stream));
+    CK(upload(S.fwd, fr.data(), fr.size(), c->stream));
+    CK(upload(S.bwd, br.data(), br.size(), c->stream));
+    if (keep_levels) {
+        c->lvl_fwd_ptr = std::move(fp);
+        c->lvl_fwd_rows = std::move(fr);
+        c->lvl_bwd_ptr = std::move(bp);
+        c->lvl_bwd_rows = std::move(br);
+    }
+    S.h_rp = std::move(rp);
+    S.h_ci = std::move(ci);
+    CK(c->done.reserve(std::max<size_t>(c->done.n, n + 1)));
+    CK(cudaMemsetAsync(c->done.p, 0, c->done.n * sizeof(unsigned), c->stream));
+    c->epoch = 0;
+    CK(cudaStreamSynchronize(c->stream));
+    return FM_OK;
+}
+
+template <typename T>
+Work<T>& work(fm_ctx* c);
+template <>
+Work<double>& work<double>(fm_ctx* c) {
+    return c->w64;
+}
+template <>
+Work<float>& work<float>(fm_ctx* c) {
+    return c->w32;
+}
+
+template <typename T>
+fm_status ensure_vectors(fm_ctx* c, uint32_t n) {
+    Work<T>& w = work<T>(c);
+    CK(w.r.reserve(n));
+    CK(w.z.reserve(n));
+    CK(w.p.reserve(n));
+    CK(w.Ap.reserve(n));
+    CK(w.t.reserve(n));
+    CK(w.b.reserve(n));
+    CK(w.x.reserve(n));
+    return FM_OK;
+}
+
+unsigned next_epoch(fm_ctx* c) {
+    if (++c->epoch == 0) c->epoch = 1;
+    return c->epoch;
+}
+
+// A linear operator for PCG: the mesh K (node-block SpMV) or a generic CSR.
+template <typename T>
+struct Op {
+    fm_ctx* c;
+    SolverCsr* S;
+    bool node_block;
+    const T* K;
+    const T* LU;
+    const T* diag;
+    T* tmp;
+    int grid_trsv;
+    void spmv(const T* x, T* y, double* dot) const {
+        T* part = reinterpret_cast<T*>(c->partials.p);
+        if (node_block)
+            fm::launch_spmv_nodes<T>(c->nn, c->nbr_ptr.p, c->nbr.p, K, x, y, part, c->counter(),
+                                     dot, c->stream);
+        else
+            fm::launch_spmv_csr<T>(S->n, S->rp.p, S->ci.p, K, x, y, part, c->counter(), dot,
+                                   c->stream);
+    }
+    void precond(const T* r, T* z) const {
+        const fm::CsrDev v = S->view();
+        fm::launch_trsv_lower_csr<T>(v, LU, r, tmp, c->done.p, next_epoch(c), c->status(),
+                                     grid_trsv, c->stream);
+        fm::launch_trsv_upper_csr<T>(v, LU, diag, tmp, z, c->done.p, next_epoch(c), c->status(),
+                                     grid_trsv, c->stream);
+    }
+};
+
+// PCG-ILU(0) with the reference's stop tests (FEM/adaptive_fem_engine.hpp:1292-1340).
+// b, x: length-n device vectors of type T; x in/out.
+template <typename T>
+fm_status pcg_core(fm_ctx* c, const Op<T>& A, uint32_t n, const T* b, T* x, double tol,
+                   int max_iter, int* iters_out, double* relres_out) {
+    Work<T>& w = work<T>(c);
+    T* part = reinterpret_cast<T*>(c->partials.p);
+    fm::DevScalars* sc = c->sc.p;
+    CK(cudaMemsetAsync(&sc->stop, 0, sizeof(unsigned), c->stream));
+    // r = b - A x
+    A.spmv(x, w.r.p, nullptr);
+    fm::launch_residual_init<T>(n, b, w.r.p, part, c->counter(), &sc->rr, c->stream);
+    TRY(sync_scalars(c));
+    TRY(check_flags(c, c->h_sc->status, "pcg"));
+    int iters = max_iter;
+    double relres = 0.0;
+    if (std::sqrt(c->h_sc->rr) < tol * 1e-3) {
+        iters = 0;
+    } else {
+        A.precond(w.r.p, w.z.p);
+        fm::launch_pcg_start<T>(n, w.r.p, w.z.p, b, w.p.p, part, c->counter(), sc, c->stream);
+        for (int it = 0; it < max_iter; ++it) {
+            A.spmv(w.p.p, w.Ap.p, &sc->pAp);
+            fm::launch_pcg_update_xr<T>(n, w.p.p, w.Ap.p, x, w.r.p, sc, c->stream);
+            A.precond(w.r.p, w.z.p);
+            fm::launch_pcg_rz<T>(n, w.r.p, w.z.p, part, c->counter(), sc, c->stream);
+            TRY(sync_scalars(c));
+            TRY(check_flags(c, c->h_sc->status, "pcg"));
+            if (c->h_sc->stop) break;  // |p.Ap| < 1e-60
+            relres = c->h_sc->relres;
+            if (relres < tol) {
+                iters = it + 1;
+                break;
+            }
+            fm::launch_pcg_update_p<T>(n, w.z.p, w.p.p, sc, c->stream);
+        }
+    }
+    if (iters_out) *iters_out = iters;
+    if (relres_out) *relres_out = relres;
+    return FM_OK;
+}
+
+template <typename T>
+fm_status ilu_core(fm_ctx* c, SolverCsr& S, const T* a, T* lu, T* diag) {
+    const fm::CsrDev v = S.view();
+    const int grid = fm::persistent_grid_ilu0_csr(c->device, sizeof(T) == 4, v);
+    fm::launch_ilu0_csr<T>(v, a, lu, diag, c->done.p, next_epoch(c), c->status(), grid,
+                           c->stream);
+    CK(cudaGetLastError());
+    return FM_OK;
+}
+
+fm_status need_mesh(fm_ctx* c) {
+    if (!c) return FM_ERR_ARG;
+    if (!c->nn) return fail(c, FM_ERR_ARG, "no mesh: call fm_set_mesh first");
+    return FM_OK;
+}
+fm_status need_material(fm_ctx* c) {
+    TRY(need_mesh(c));
+    if (!c->has_mat) return fail(c, FM_ERR_ARG, "no material: call fm_set_material first");
+    return FM_OK;
+}
+
+template <typename T>
+fm_status ensure_matrix(fm_ctx* c) {
+    Work<T>& w = work<T>(c);
+    CK(w.K.reserve(c->nnz));
+    CK(w.LU.reserve(c->nnz));
+    CK(w.diag.reserve(c->n));
+    return ensure_vectors<T>(c, c->n);
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+fm_status fm_create(fm_ctx** out, int device, void* stream) {
+    if (!out) return FM_ERR_ARG;
+    *out = nullptr;
+    fm_ctx* c = nullptr;
+    try {
+        c = new fm_ctx;
+    } catch (const std::bad_alloc&) {
+        return FM_ERR_OOM;
+    }
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete c;
+        return FM_ERR_CUDA;
+    }
+    if (stream) {
+        c->stream = static_cast<cudaStream_t>(stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete c;
+            return FM_ERR_CUDA;
+        }
+        c->own_stream = true;
+    }
+    if (c->sc.reserve(1) != cudaSuccess || c->partials.reserve(8192) != cudaSuccess ||
+        cudaMallocHost(&c->h_sc, sizeof(fm::DevScalars)) != cudaSuccess) {
+        fm_destroy(c);
+        return FM_ERR_OOM;
+    }
+    cudaMemsetAsync(c->sc.p, 0, sizeof(fm::DevScalars), c->stream);
+    cudaMemsetAsync(c->partials.p, 0, c->partials.n * sizeof(double), c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        fm_destroy(c);
+        return FM_ERR_CUDA;
+    }
+    c->grid_trsv64 = fm::persistent_grid_trsv_csr(device, false);
+    c->grid_trsv32 = fm::persistent_grid_trsv_csr(device, true);
+    *out = c;
+    return FM_OK;
+}
+
+void fm_destroy(fm_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->h_sc) cudaFreeHost(c->h_sc);
+    bool own = c->own_stream;
+    cudaStream_t s = c->stream;
+    delete c;
+    if (own && s) cudaStreamDestroy(s);
+}
+
+fm_status fm_last_error(const fm_ctx* c, char* buf, size_t len) {
+    if (!c || !buf || !len) return FM_ERR_ARG;
+    std::snprintf(buf, len, "%s", c->err.c_str());
+    return FM_OK;
+}
+
+fm_status fm_get_flags(fm_ctx* c, uint32_t* flags) {
+    if (!c || !flags) return FM_ERR_ARG;
+    return device_flags(c, flags);
+}
+
+fm_status fm_clear_flags(fm_ctx* c) {
+    if (!c) return FM_ERR_ARG;
+    CK(cudaMemsetAsync(&c->sc.p->status, 0, sizeof(unsigned), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FM_OK;
+}
+
+fm_status fm_sizes(const fm_ctx* c, uint32_t* n_nodes, uint32_t* n_elems, uint32_t* n_dofs,
+                   uint64_t* nnz) {
+    if (!c) return FM_ERR_ARG;
+    if (n_nodes) *n_nodes = c->nn;
+    if (n_elems) *n_elems = c->ne;
+    if (n_dofs) *n_dofs = c->n;
+    if (nnz) *nnz = c->nnz;
+    return FM_OK;
+}
+
+fm_status fm_unit_cube_sizes(int N, uint32_t* n_nodes, uint32_t* n_elems) {
+    if (N < 1 || N > 1200 || !n_nodes || !n_elems) return FM_ERR_ARG;
+    const uint64_t s = (uint64_t)N + 1;
+    *n_nodes = (uint32_t)(s * s * s);
+    *n_elems = (uint32_t)(6ull * N * N * N);
+    return FM_OK;
+}
+
+fm_status fm_unit_cube(int N, double* xyz, uint32_t* conn) {
+    if (N < 1 || N > 1200 || !xyz || !conn) return FM_ERR_ARG;
+    fm::unit_cube(N, xyz, conn);
+    return FM_OK;
+}
+
+fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n_elems,
+                      const uint32_t* conn, const double* elem_volume) {
+    if (!c) return FM_ERR_ARG;
+    if (!xyz || !conn || !n_nodes || !n_elems) return fail(c, FM_ERR_ARG, "empty mesh");
+    if (n_nodes >= (1u << 30)) return fail(c, FM_ERR_ARG, "n_nodes too large");
+    try {
+        CK(cudaSetDevice(c->device));
+        for (size_t q = 0; q < 4 * (size_t)n_elems; ++q)
+            if (conn[q] >= n_nodes)
+                return fail(c, FM_ERR_ARG, "conn[%zu] = %u out of range", q, conn[q]);
+        c->nn = n_nodes;
+        c->ne = n_elems;
+        c->n = 3 * n_nodes;
+        c->h_xyz.assign(xyz, xyz + 3 * (size_t)n_nodes);
+        c->h_conn.assign(conn, conn + 4 * (size_t)n_elems);
+        c->h_skip.assign(n_elems, 0);
+        if (elem_volume)
+            for (uint32_t e = 0; e < n_elems; ++e) c->h_skip[e] = !(elem_volume[e] >= 1e-30);
+        c->graph = fm::build_node_graph(n_nodes, n_elems, conn);
+        c->inc = fm::build_incidence(n_nodes, n_elems, conn);
+        if (c->graph.max_deg > 32 || c->inc.max_inc > 32)
+            return fail(c, FM_ERR_LIMITS,
+                        "mesh valence beyond kernel limits (max neighbours %u, max incident "
+                        "tets %u; both must be <= 32)",
+                        c->graph.max_deg, c->inc.max_inc);
+        const uint64_t nnz = 9ull * c->graph.ptr[n_nodes];
+        if (nnz >= (1ull << 32)) return fail(c, FM_ERR_LIMITS, "nnz %llu exceeds 32-bit CSR",
+                                             (unsigned long long)nnz);
+        c->nnz = nnz;
+        std::vector<uint4> cw(n_elems);
+        for (uint32_t e = 0; e < n_elems; ++e) {
+            const uint32_t* q = conn + 4 * (size_t)e;
+            cw[e] = make_uint4(q[0] | (c->h_skip[e] ? 0x80000000u : 0u), q[1], q[2], q[3]);
+        }
+        CK(upload(c->xyz, xyz, 3 * (size_t)n_nodes, c->stream));
+        CK(upload(c->conn, cw.data(), n_elems, c->stream));
+        CK(upload(c->nbr_ptr, c->graph.ptr.data(), c->graph.ptr.size(), c->stream));
+        CK(upload(c->nbr, c->graph.nbr.data(), c->graph.nbr.size(), c->stream));
+        CK(upload(c->inc_ptr, c->inc.ptr.data(), c->inc.ptr.size(), c->stream));
+        CK(upload(c->inc_e, c->inc.elem.data(), c->inc.elem.size(), c->stream));
+        std::vector<uint32_t> rp(c->n + 1), ci(nnz);
+        fm::csr_row_ptr(c->graph, rp.data());
+        fm::csr_solve_cols(c->graph, ci.data());
+        TRY(setup_solver_csr(c, c->fem, c->n, std::move(rp), std::move(ci), true));
+        c->w64.factor_valid = c->w32.factor_valid = false;
+        c->has_bc = false;
+        c->has_mat = false;
+        c->ref_slot.release();
+        CK(c->vec_a.reserve(c->n));
+        CK(c->vec_b.reserve(c->n));
+        CK(cudaStreamSynchronize(c->stream));
+    } catch (const std::bad_alloc&) {
+        return fail(c, FM_ERR_OOM, "host allocation failed in fm_set_mesh");
+    }
+    return FM_OK;
+}
+
+fm_status fm_build_pattern(fm_ctx* c, fm_pattern kind, uint32_t* row_ptr_out,
+                           uint32_t* col_idx_out, int32_t* slot_map_out) {
+    TRY(need_mesh(c));
+    try {
+        std::vector<uint32_t> ref_cols;
+        const uint32_t* cols = c->fem.h_ci.data();
+        if (kind == FM_PATTERN_REFERENCE) {
+            ref_cols.resize(c->nnz);
+            fm::csr_reference_cols(c->graph, ref_cols.data());
+            cols = ref_cols.data();
+        } else if (kind != FM_PATTERN_SOLVE) {
+            return fail(c, FM_ERR_ARG, "unknown pattern kind %d", (int)kind);
+        }
+        if (row_ptr_out)
+            std::memcpy(row_ptr_out, c->fem.h_rp.data(), sizeof(uint32_t) * (c->n + 1));
+        if (col_idx_out) std::memcpy(col_idx_out, cols, sizeof(uint32_t) * c->nnz);
+        if (slot_map_out)
+            fm::slot_map(c->fem.h_rp.data(), cols, c->ne, c->h_conn.data(), slot_map_out);
+    } catch (const std::bad_alloc&) {
+        return fail(c, FM_ERR_OOM, "host allocation failed in fm_build_pattern");
+    }
+    return FM_OK;
+}
+
+fm_status fm_set_material(fm_ctx* c, double E, double nu, const double* E_elem) {
+    TRY(need_mesh(c));
+    if (!(nu > -1.0 && nu < 0.5)) return fail(c, FM_ERR_ARG, "nu must be in (-1, 0.5)");
+    c->nu = nu;
+    // mu, lambda exactly as the reference forms them (FEM/adaptive_fem_engine.hpp:81-82)
+    c->mu_s = E / (2.0 * (1.0 + nu));
+    c->lam_s = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    c->c_mu = 1.0 / (2.0 * (1.0 + nu));
+    c->c_lam = nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    const double one_m = 1.0 - 2.0 * nu;
+    c->inv_cnu = 1.0 / (one_m < 0.1 ? 0.1 : one_m);
+    if (E_elem) {
+        CK(upload(c->m0, E_elem, c->ne, c->stream));
+        c->mat_mode = 1;
+    } else {
+        c->mat_mode = 0;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    c->has_mat = true;
+    return FM_OK;
+}
+
+fm_status fm_set_material_lame(fm_ctx* c, const double* mu_elem, const double* lambda_elem,
+                               double nu) {
+    TRY(need_mesh(c));
+    if (!mu_elem || !lambda_elem) return fail(c, FM_ERR_ARG, "mu/lambda arrays required");
+    if (!(nu > -1.0 && nu < 0.5)) return fail(c, FM_ERR_ARG, "nu must be in (-1, 0.5)");
+    c->nu = nu;
+    const double one_m = 1.0 - 2.0 * nu;
+    c->inv_cnu = 1.0 / (one_m < 0.1 ? 0.1 : one_m);
+    CK(upload(c->m0, mu_elem, c->ne, c->stream));
+    CK(upload(c->m1, lambda_elem, c->ne, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->mat_mode = 2;
+    c->has_mat = true;
+    return FM_OK;
+}
+
+fm_status fm_set_bc(fm_ctx* c, const uint8_t* dof_mask, const double* dof_value) {
+    TRY(need_mesh(c));
+    if (!dof_mask) {
+        c->has_bc = false;
+        return FM_OK;
+    }
+    std::vector<uint8_t> m(dof_mask, dof_mask + c->n);
+    for (auto& v : m) v = v ? 1 : 0;
+    CK(upload(c->mask, m.data(), c->n, c->stream));
+    c->has_bcval = dof_value != nullptr;
+    if (dof_value) CK(upload(c->bcval, dof_value, c->n, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->has_bc = true;
+    return FM_OK;
+}
+
+fm_status fm_elements(fm_ctx* c, uint32_t n, const double* x, const double* u, const double* E,
+                      double nu, double* K, double* f) {
+    if (!c || !x || !u || !E || !K || !f) return fail(c, FM_ERR_ARG, "null argument");
+    fm::launch_elements(n, x, u, E, nu, K, f, c->status(), c->stream);
+    CK(cudaGetLastError());
+    uint32_t flags;
+    TRY(device_flags(c, &flags));
+    return check_flags(c, flags, "fm_elements");
+}
+
+fm_status fm_assemble(fm_ctx* c, const double* u, void* K, double* f, fm_precision prec,
+                      int apply_bc) {
+    TRY(need_material(c));
+    if (!u) return fail(c, FM_ERR_ARG, "u is null");
+    const fm::MeshDev m = mesh_view(c);
+    if (prec == FM_FP64) {
+        TRY(ensure_matrix<double>(c));
+        double* Kd = K ? static_cast<double*>(K) : c->w64.K.p;
+        fm::launch_assemble(m, u, Kd, f, nullptr, apply_bc && c->has_bc, c->status(), c->stream);
+        c->w64.factor_valid = false;
+    } else if (prec == FM_MIXED) {
+        TRY(ensure_matrix<float>(c));
+        float* Kf = K ? static_cast<float*>(K) : c->w32.K.p;
+        fm::launch_assemble(m, u, Kf, f, nullptr, apply_bc && c->has_bc, c->status(), c->stream);
+        c->w32.factor_valid = false;
+    } else {
+        return fail(c, FM_ERR_ARG, "unknown precision");
+    }
+    CK(cudaGetLastError());
+    return FM_OK;
+}
+
+fm_status fm_assemble_host(fm_ctx* c, const double* u_host, double* K_host, double* f_host) {
+    TRY(need_material(c));
+    if (!u_host) return fail(c, FM_ERR_ARG, "u is null");
+    TRY(ensure_matrix<double>(c));
+    CK(cudaMemcpyAsync(c->vec_a.p, u_host, sizeof(double) * c->n, cudaMemcpyHostToDevice,
+                       c->stream));
+    const fm::MeshDev m = mesh_view(c);
+    fm::launch_assemble(m, c->vec_a.p, c->w64.K.p, c->vec_b.p, nullptr, 0, c->status(),
+                        c->stream);
+    CK(cudaGetLastError());
+    c->w64.factor_valid = false;
+    if (K_host)
+        CK(cudaMemcpyAsync(K_host, c->w64.K.p, sizeof(double) * c->nnz, cudaMemcpyDeviceToHost,
+                           c->stream));
+    if (f_host)
+        CK(cudaMemcpyAsync(f_host, c->vec_b.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost,
+                           c->stream));
+    uint32_t flags;
+    TRY(device_flags(c, &flags));
+    return check_flags(c, flags, "fm_assemble_host");
+}
+
+fm_status fm_residual(fm_ctx* c, const double* u, double* f) {
+    TRY(need_material(c));
+    if (!u || !f) return fail(c, FM_ERR_ARG, "null argument");
+    const fm::MeshDev m = mesh_view(c);
+    fm::launch_assemble(m, u, static_cast<double*>(nullptr), f, nullptr, 0, c->status(),
+                        c->stream);
+    CK(cudaGetLastError());
+    return FM_OK;
+}
+
+fm_status fm_assemble_reference_pattern(fm_ctx* c, const double* u, double* K, double* f) {
+    TRY(need_material(c));
+    if (!u || !K || !f) return fail(c, FM_ERR_ARG, "null argument");
+    try {
+        if (!c->ref_slot.p) {
+            std::vector<uint32_t> cols(c->nnz);
+            fm::csr_reference_cols(c->graph, cols.data());
+            std::vector<int32_t> slot(144 * (size_t)c->ne);
+            fm::slot_map(c->fem.h_rp.data(), cols.data(), c->ne, c->h_conn.data(), slot.data());
+            CK(upload(c->ref_slot, slot.data(), slot.size(), c->stream));
+        }
+    } catch (const std::bad_alloc&) {
+        return fail(c, FM_ERR_OOM, "host allocation failed");
+    }
+    CK(c->ke_scratch.reserve(144 * (size_t)c->ne));
+    CK(cudaMemsetAsync(K, 0, sizeof(double) * c->nnz, c->stream));
+    CK(cudaMemsetAsync(f, 0, sizeof(double) * c->n, c->stream));
+    fm::launch_assemble_slotmap(mesh_view(c), u, c->ref_slot.p, K, f, c->ke_scratch.p,
+                                c->status(), c->stream);
+    CK(cudaGetLastError());
+    uint32_t flags;
+    TRY(device_flags(c, &flags));
+    return check_flags(c, flags, "fm_assemble_reference_pattern");
+}
+
+fm_status fm_levels(fm_ctx* c, uint32_t* fwd_ptr, uint32_t* fwd_rows, uint32_t* bwd_ptr,
+                    uint32_t* bwd_rows, uint32_t* n_fwd, uint32_t* n_bwd) {
+    TRY(need_mesh(c));
+    if (fwd_ptr) std::copy(c->lvl_fwd_ptr.begin(), c->lvl_fwd_ptr.end(), fwd_ptr);
+    if (fwd_rows) std::copy(c->lvl_fwd_rows.begin(), c->lvl_fwd_rows.end(), fwd_rows);
+    if (bwd_ptr) std::copy(c->lvl_bwd_ptr.begin(), c->lvl_bwd_ptr.end(), bwd_ptr);
+    if (bwd_rows) std::copy(c->lvl_bwd_rows.begin(), c->lvl_bwd_rows.end(), bwd_rows);
+    if (n_fwd) *n_fwd = (uint32_t)c->lvl_fwd_ptr.size() - 1;
+    if (n_bwd) *n_bwd = (uint32_t)c->lvl_bwd_ptr.size() - 1;
+    return FM_OK;
+}
+
+fm_status fm_ilu0(fm_ctx* c, fm_precision prec) {
+    TRY(need_mesh(c));
+    if (prec == FM_FP64) {
+        TRY(ensure_matrix<double>(c));
+        TRY(ilu_core<double>(c, c->fem, c->w64.K.p, c->w64.LU.p, c->w64.diag.p));
+        c->w64.factor_valid = true;
+    } else if (prec == FM_MIXED) {
+        TRY(ensure_matrix<float>(c));
+        TRY(ilu_core<float>(c, c->fem, c->w32.K.p, c->w32.LU.p, c->w32.diag.p));
+        c->w32.factor_valid = true;
+    } else {
+        return fail(c, FM_ERR_ARG, "unknown precision");
+    }
+    uint32_t flags;
+    TRY(device_flags(c, &flags));
+    return check_flags(c, flags, "fm_ilu0");
+}
+
+fm_status fm_get_ilu0(fm_ctx* c, double* LU, double* diag) {
+    TRY(need_mesh(c));
+    if (!c->w64.factor_valid) return fail(c, FM_ERR_ARG, "no FP64 factorization: call fm_ilu0");
+    if (LU)
+        CK(cudaMemcpyAsync(LU, c->w64.LU.p, sizeof(double) * c->nnz, cudaMemcpyDeviceToHost,
+                           c->stream));
+    if (diag)
+        CK(cudaMemcpyAsync(diag, c->w64.diag.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost,
+                           c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FM_OK;
+}
+
+fm_status fm_ilu0_apply(fm_ctx* c, const double* r, double* y) {
+    TRY(need_mesh(c));
+    if (!c->w64.factor_valid) return fail(c, FM_ERR_ARG, "no FP64 factorization: call fm_ilu0");
+    if (!r || !y) return fail(c, FM_ERR_ARG, "null argument");
+    Op<double> A{c, &c->fem, true, c->w64.K.p, c->w64.LU.p, c->w64.diag.p, c->w64.t.p,
+                 c->grid_trsv64};
+    A.precond(r, y);
+    CK(cudaGetLastError());
+    uint32_t flags;
+    TRY(device_flags(c, &flags));
+    return check_flags(c, flags, "fm_ilu0_apply");
+}
+
+fm_status fm_spmv(fm_ctx* c, const double* x, double* y) {
+    TRY(need_mesh(c));
+    if (!x || !y || !c->w64.K.p) return fail(c, FM_ERR_ARG, "null argument or no K");
+    Op<double> A{c, &c->fem, true, c->w64.K.p, nullptr, nullptr, nullptr, 0};
+    A.spmv(x, y, nullptr);
+    CK(cudaGetLastError());
+    return FM_OK;
+}
+
+fm_status fm_pcg(fm_ctx* c, const double* b, double* x, double tol, int max_iter, int* iters,
+                 double* relres, fm_precision prec) {
+    TRY(need_mesh(c));
+    if (!b || !x || max_iter < 0) return fail(c, FM_ERR_ARG, "bad argument");
+    if (prec == FM_FP64) {
+        if (!c->w64.factor_valid) return fail(c, FM_ERR_ARG, "call fm_ilu0(FM_FP64) first");
+        Op<double> A{c, &c->fem, true, c->w64.K.p, c->w64.LU.p, c->w64.diag.p, c->w64.t.p,
+                     c->grid_trsv64};
+        return pcg_core<double>(c, A, c->n, b, x, tol, max_iter, iters, relres);
+    }
+    if (prec != FM_MIXED) return fail(c, FM_ERR_ARG, "unknown precision");
+    if (!c->w32.factor_valid) return fail(c, FM_ERR_ARG, "call fm_ilu0(FM_MIXED) first");
+    // FP32 inner solve on b/||b||; x returned in FP64
+    fm::launch_norm2(c->n, b, c->partials.p, c->counter(), &c->sc.p->norm2, c->stream);
+    TRY(sync_scalars(c));
+    const double s = std::sqrt(c->h_sc->norm2);
+    if (s == 0.0) {
+        if (iters) *iters = 0;
+        if (relres) *relres = 0.0;
+        return FM_OK;
+    }
+    fm::launch_to_f32_scaled(c->n, b, 1.0 / s, c->w32.b.p, c->w32.x.p, c->stream);
+    Op<float> A{c, &c->fem, true, c->w32.K.p, c->w32.LU.p, c->w32.diag.p, c->w32.t.p,
+                c->grid_trsv32};
+    TRY(pcg_core<float>(c, A, c->n, c->w32.b.p, c->w32.x.p, tol, max_iter, iters, relres));
+    fm::launch_axpy_u_f32(c->n, c->w32.x.p, s, x, c->stream);
+    CK(cudaGetLastError());
+    return FM_OK;
+}
+
+fm_status fm_csr_pcg_ilu0(fm_ctx* c, uint32_t n, const uint32_t* row_ptr,
+                          const uint32_t* col_idx, const double* val, const double* b,
+                          double* x, double tol, int max_iter, int* iters, double* relres) {
+    if (!c || !row_ptr || !col_idx || !val || !b || !x || n == 0)
+        return fail(c, FM_ERR_ARG, "bad argument");
+    try {
+        const uint64_t nnz = row_ptr[n];
+        // sort columns per row (values follow), as the reference's symbolic
+        // phase sorts its L/U patterns
+        std::vector<uint32_t> rp(row_ptr, row_ptr + n + 1), ci(col_idx, col_idx + nnz);
+        std::vector<double> v(val, val + nnz);
+        std::vector<std::pair<uint32_t, double>> row;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (rp[i + 1] < rp[i] || rp[i + 1] > nnz)
+                return fail(c, FM_ERR_ARG, "row_ptr not monotone at row %u", i);
+            row.clear();
+            for (uint32_t k = rp[i]; k < rp[i + 1]; ++k) {
+                if (ci[k] >= n) return fail(c, FM_ERR_ARG, "column %u out of range", ci[k]);
+                row.emplace_back(ci[k], v[k]);
+            }
+            std::stable_sort(row.begin(), row.end(),
+                             [](const auto& a, const auto& b2) { return a.first < b2.first; });
+            for (size_t q = 0; q < row.size(); ++q) {
+                ci[rp[i] + q] = row[q].first;
+                v[rp[i] + q] = row[q].second;
+            }
+        }
+        if (c->gen.n != n || c->gen.h_rp != rp || c->gen.h_ci != ci)
+            TRY(setup_solver_csr(c, c->gen, n, std::move(rp), std::move(ci), false));
+        CK(upload(c->gen_K, v.data(), nnz, c->stream));
+        CK(c->gen_LU.reserve(nnz));
+        CK(c->gen_diag.reserve(n));
+        TRY(ensure_vectors<double>(c, n));
+        CK(c->vec_a.reserve(n));
+        CK(c->vec_b.reserve(n));
+        CK(cudaMemcpyAsync(c->vec_a.p, b, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->vec_b.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+        TRY(ilu_core<double>(c, c->gen, c->gen_K.p, c->gen_LU.p, c->gen_diag.p));
+        Op<double> A{c, &c->gen, false, c->gen_K.p, c->gen_LU.p, c->gen_diag.p, c->w64.t.p,
+                     c->grid_trsv64};
+        TRY(pcg_core<double>(c, A, n, c->vec_a.p, c->vec_b.p, tol, max_iter, iters, relres));
+        CK(cudaMemcpyAsync(x, c->vec_b.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    } catch (const std::bad_alloc&) {
+        return fail(c, FM_ERR_OOM, "host allocation failed");
+    }
+    return FM_OK;
+}
+
+fm_status fm_newton_step(fm_ctx* c, double* u, double load_frac, double rtol, double atol,
+                         double inner_tol, int max_newton, int max_pcg, int line_search,
+                         double ls_c, fm_precision prec, int* newton_iters, int* pcg_iters,
+                         double* final_relres) {
+    TRY(need_material(c));
+    if (!u || max_newton < 1 || line_search < 0) return fail(c, FM_ERR_ARG, "bad argument");
+    if (prec != FM_FP64 && prec != FM_MIXED) return fail(c, FM_ERR_ARG, "unknown precision");
+    const bool mixed = prec == FM_MIXED;
+    if (mixed) TRY(ensure_matrix<float>(c));
+    else TRY(ensure_matrix<double>(c));
+    if (line_search) CK(c->vec_c.reserve(c->n));
+    const fm::MeshDev m = mesh_view(c);
+    double* R = c->vec_a.p;
+    double* du = c->vec_b.p;
+    if (c->has_bc)
+        fm::launch_set_bc_values(c->n, c->mask.p, c->has_bcval ? c->bcval.p : nullptr, load_frac,
+                                 u, c->stream);
+    int n_newton = 0, n_pcg = 0;
+    double r0 = 0.0, last_rel = 0.0;
+    bool conv = false;
+    for (int it = 0; it < max_newton; ++it) {
+        if (mixed)
+            fm::launch_assemble(m, u, c->w32.K.p, nullptr, R, 1, c->status(), c->stream);
+        else
+            fm::launch_assemble(m, u, c->w64.K.p, nullptr, R, 1, c->status(), c->stream);
+        fm::launch_norm2(c->n, R, c->partials.p, c->counter(), &c->sc.p->norm2, c->stream);
+        TRY(sync_scalars(c));
+        TRY(check_flags(c, c->h_sc->status, "newton assembly"));
+        const double rn = std::sqrt(c->h_sc->norm2);
+        if (it == 0) r0 = rn;
+        last_rel = r0 > 0 ? rn / r0 : 0.0;
+        if (rn == 0.0 || rn < rtol * r0 || rn < atol) {
+            conv = true;
+            break;
+        }
+        int its = 0;
+        if (mixed) {
+            // FP32 tangent/ILU(0)/PCG on R/||R||; the step is rescaled in FP64
+            TRY(ilu_core<float>(c, c->fem, c->w32.K.p, c->w32.LU.p, c->w32.diag.p));
+            fm::launch_to_f32_scaled(c->n, R, 1.0 / rn, c->w32.b.p, c->w32.x.p, c->stream);
+            Op<float> A{c, &c->fem, true, c->w32.K.p, c->w32.LU.p, c->w32.diag.p, c->w32.t.p,
+                        c->grid_trsv32};
+            TRY(pcg_core<float>(c, A, c->n, c->w32.b.p, c->w32.x.p, inner_tol, max_pcg, &its,
+                                nullptr));
+            if (line_search) fm::launch_f32_to_f64_scaled(c->n, c->w32.x.p, rn, du, c->stream);
+            else fm::launch_axpy_u_f32(c->n, c->w32.x.p, rn, u, c->stream);
+        } else {
+            TRY(ilu_core<double>(c, c->fem, c->w64.K.p, c->w64.LU.p, c->w64.diag.p));
+            CK(cudaMemsetAsync(du, 0, sizeof(double) * c->n, c->stream));
+            Op<double> A{c, &c->fem, true, c->w64.K.p, c->w64.LU.p, c->w64.diag.p, c->w64.t.p,
+                         c->grid_trsv64};
+            TRY(pcg_core<double>(c, A, c->n, R, du, inner_tol, max_pcg, &its, nullptr));
+            if (!line_search) fm::launch_axpy_u(c->n, du, u, c->stream);
+        }
+        if (line_search) {
+            // Armijo backtracking on the residual norm with residual-only
+            // re-assembly at each trial point
+            double alpha = 1.0;
+            for (int bt = 0; bt < line_search; ++bt) {
+                fm::launch_trial(c->n, u, alpha, du, c->vec_c.p, c->stream);
+                fm::launch_assemble(m, c->vec_c.p, static_cast<double*>(nullptr), nullptr, R, 0,
+                                    c->status(), c->stream);
+                fm::launch_norm2(c->n, R, c->partials.p, c->counter(), &c->sc.p->norm2,
+                                 c->stream);
+                TRY(sync_scalars(c));
+                if (std::sqrt(c->h_sc->norm2) <= (1.0 - ls_c * alpha) * rn) break;
+                if (bt + 1 < line_search) alpha *= 0.5;
+            }
+            fm::launch_trial(c->n, u, alpha, du, u, c->stream);
+        }
+        CK(cudaGetLastError());
+        n_pcg += its;
+        ++n_newton;
+    }
+    c->w64.factor_valid = c->w32.factor_valid = false;
+    CK(cudaStreamSynchronize(c->stream));
+    if (newton_iters) *newton_iters = n_newton;
+    if (pcg_iters) *pcg_iters = n_pcg;
+    if (final_relres) *final_relres = last_rel;
+    if (!conv) return fail(c, FM_ERR_NOT_CONVERGED, "Newton hit max_newton=%d", max_newton);
+    return FM_OK;
+}
+
+fm_status fm_newton_solve(fm_ctx* c, double* u, int first_step, int n_steps, double rtol,
+                          double atol, double inner_tol, int max_newton, int max_pcg,
+                          fm_precision prec, int* newton_iters, int* pcg_iters,
+                          double* final_relres) {
+    TRY(need_material(c));
+    if (!u || n_steps < 1 || first_step < 1 || first_step > n_steps)
+        return fail(c, FM_ERR_ARG, "bad load-step range");
+    int tn = 0, tp = 0;
+    double rel = 0.0;
+    fm_status worst = FM_OK;
+    for (int s = first_step; s <= n_steps; ++s) {
+        int nn = 0, np = 0;
+        fm_status st = fm_newton_step(c, u, (double)s / (double)n_steps, rtol, atol, inner_tol,
+                                      max_newton, max_pcg, 0, 0.0, prec, &nn, &np, &rel);
+        tn += nn;
+        tp += np;
+        if (st == FM_ERR_NOT_CONVERGED) worst = st;
+        else if (st != FM_OK) return st;
+    }
+    if (newton_iters) *newton_iters = tn;
+    if (pcg_iters) *pcg_iters = tp;
+    if (final_relres) *final_relres = rel;
+    if (worst != FM_OK) return fail(c, worst, "a load step hit max_newton=%d", max_newton);
+    return FM_OK;
+}
+
+fm_status fm_csr_ilu0(fm_ctx* c, uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx,
+                      const double* val, double* LU_out, double* diag_out) {
+    if (!c || !row_ptr || !col_idx || !val || n == 0) return fail(c, FM_ERR_ARG, "bad argument");
+    try {
+        const uint64_t nnz = row_ptr[n];
+        std::vector<uint32_t> rp(row_ptr, row_ptr + n + 1), ci(col_idx, col_idx + nnz);
+        std::vector<double> v(val, val + nnz);
+        std::vector<uint32_t> perm(nnz);  // sorted slot -> caller slot
+        for (uint32_t i = 0; i < n; ++i) {
+            if (rp[i + 1] < rp[i] || rp[i + 1] > nnz)
+                return fail(c, FM_ERR_ARG, "row_ptr not monotone at row %u", i);
+            for (uint32_t k = rp[i]; k < rp[i + 1]; ++k) {
+                if (col_idx[k] >= n) return fail(c, FM_ERR_ARG, "column out of range");
+                perm[k] = k;
+            }
+            std::stable_sort(perm.begin() + rp[i], perm.begin() + rp[i + 1],
+                             [&](uint32_t a, uint32_t b) { return col_idx[a] < col_idx[b]; });
+            for (uint32_t k = rp[i]; k < rp[i + 1]; ++k) {
+                ci[k] = col_idx[perm[k]];
+                v[k] = val[perm[k]];
+            }
+        }
+        if (c->gen.n != n || c->gen.h_rp != rp || c->gen.h_ci != ci)
+            TRY(setup_solver_csr(c, c->gen, n, std::move(rp), std::move(ci), false));
+        CK(upload(c->gen_K, v.data(), nnz, c->stream));
+        CK(c->gen_LU.reserve(nnz));
+        CK(c->gen_diag.reserve(n));
+        TRY(ilu_core<double>(c, c->gen, c->gen_K.p, c->gen_LU.p, c->gen_diag.p));
+        std::vector<double> lu(nnz);
+        CK(cudaMemcpyAsync(lu.data(), c->gen_LU.p, sizeof(double) * nnz, cudaMemcpyDeviceToHost,
+                           c->stream));
+        if (diag_out)
+            CK(cudaMemcpyAsync(diag_out, c->gen_diag.p, sizeof(double) * n,
+                               cudaMemcpyDeviceToHost, c->stream));
+        uint32_t flags;
+        TRY(device_flags(c, &flags));
+        TRY(check_flags(c, flags, "fm_csr_ilu0"));
+        if (LU_out)
+            for (uint64_t k = 0; k < nnz; ++k) LU_out[perm[k]] = lu[k];
+    } catch (const std::bad_alloc&) {
+        return fail(c, FM_ERR_OOM, "host allocation failed");
+    }
+    return FM_OK;
+}
+
+fm_status fm_exact_apply(fm_ctx* c, const double*, const double*, double*, int) {
+    return fail(c, FM_ERR_ARG, "fm_exact_apply: not built yet");
+}
+
+fm_status fm_adjoint(fm_ctx* c, const double*, const double*, double*, double*, double*, double,
+                     double, int, fm_precision, int*, int*) {
+    return fail(c, FM_ERR_ARG, "fm_adjoint: not built yet");
+}
+
+}  // extern "C"

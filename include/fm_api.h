@@ -1,0 +1,246 @@
+/*
+ * fm_api.h — C ABI of the B200 FlexMesh hot path (libflexmesh_b200.so).
+ *
+ * One Newton iteration of FlexMesh's finite-strain solve, on one GPU:
+ *   compressible Neo-Hookean force + 12x12 tangent per tetrahedron,
+ *   scatter into a CSR global stiffness (no atomics: each CSR row block is
+ *   written once by the warp that owns its node),
+ *   Dirichlet elimination, ILU(0) factorization and ILU(0)-preconditioned CG
+ *   (SpMV + dependency-ordered triangular solves), Newton load stepping,
+ *   and the adjoint for per-element material gradients.
+ *
+ * Conventions
+ *   - Plain C; no exceptions cross the boundary; every call returns fm_status.
+ *   - Host arrays are caller-owned and only read/written during the call.
+ *     Arguments named *_dev are device pointers on the context's device.
+ *   - Node coordinates and DOF vectors are interleaved per node:
+ *     xyz[3*n+d], u[3*n+d] (the reference's MeshNode order, DOF 3n+d).
+ *     Connectivity is conn[4*e+v].
+ *   - All device work is ordered on the context's stream; calls that return
+ *     scalars (iteration counts, norms, status) synchronize that stream.
+ *   - A context is not thread-safe; use one context per host thread.
+ *   - Kernels never trap: device-side problems set a status word that the
+ *     calls translate into FM_ERR_* codes (see fm_last_error for text).
+ *
+ * Every entry point cites the reference interface it replaces
+ * (file:line in the FlexMesh sources).
+ */
+#ifndef FM_API_H
+#define FM_API_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fm_ctx fm_ctx;
+
+typedef enum {
+    FM_OK = 0,
+    FM_ERR_ARG = 1,            /* bad argument or call order */
+    FM_ERR_CUDA = 2,           /* CUDA runtime error */
+    FM_ERR_OOM = 3,            /* device allocation failed */
+    FM_ERR_NONFINITE = 4,      /* NaN/Inf produced (element or solver) */
+    FM_ERR_ZERO_PIVOT = 5,     /* reserved: pivots are perturbed, not fatal */
+    FM_ERR_INVERTED = 6,       /* reserved: det F <= 0 is reported as a flag */
+    FM_ERR_TIMEOUT = 7,        /* a bounded device wait expired */
+    FM_ERR_NOT_CONVERGED = 8,  /* Newton/PCG stopped at its iteration cap */
+    FM_ERR_LIMITS = 9          /* mesh valence beyond the kernels' limits */
+} fm_status;
+
+typedef enum { FM_FP64 = 0, FM_MIXED = 1 } fm_precision;
+
+/* FM_PATTERN_REFERENCE: the reference's CSR exactly as its builder writes it
+ * (FEM/adaptive_fem_engine.hpp:1069-1120, including its column-fill defect).
+ * FM_PATTERN_SOLVE: same row_ptr, every row of node n lists all 3|nb(n)|
+ * columns ascending (the fill the Newton/PCG path needs). */
+typedef enum { FM_PATTERN_REFERENCE = 0, FM_PATTERN_SOLVE = 1 } fm_pattern;
+
+/* Device status flags accumulated since the last fm_clear_flags. */
+enum {
+    FM_FLAG_NONFINITE = 1u << 0, /* NaN/Inf in an element or solver value */
+    FM_FLAG_INVERTED = 1u << 1,  /* det F <= 0 met in an element */
+    FM_FLAG_J_CLAMPED = 1u << 2, /* det F < 0.01, ln J clamped as the reference does */
+    FM_FLAG_PIVOT = 1u << 3,     /* an ILU(0) pivot was perturbed (|u_ii| < 1e-12) */
+    FM_FLAG_TIMEOUT = 1u << 4,   /* a bounded dependency wait expired */
+    FM_FLAG_BREAKDOWN = 1u << 5  /* PCG |p.Ap| < 1e-60 */
+};
+
+/* ---- context ----------------------------------------------------------- */
+/* cuda_stream: a cudaStream_t, or NULL to let the context create its own. */
+fm_status fm_create(fm_ctx** ctx, int device, void* cuda_stream);
+void fm_destroy(fm_ctx* ctx);
+/* Text of the last error on this context (always NUL-terminated). */
+fm_status fm_last_error(const fm_ctx* ctx, char* buf, size_t len);
+fm_status fm_get_flags(fm_ctx* ctx, uint32_t* flags);
+fm_status fm_clear_flags(fm_ctx* ctx);
+/* Size queries after fm_set_mesh: DOFs, CSR nonzeros, node neighbours. */
+fm_status fm_sizes(const fm_ctx* ctx, uint32_t* n_nodes, uint32_t* n_elems, uint32_t* n_dofs,
+                   uint64_t* nnz);
+
+/* ---- A1: unit-cube generator (host only) ---------------------------------
+ * Replaces generate_unit_cube_mesh, FEM/adaptive_fem_engine.hpp:2219-2294:
+ * (N+1)^3 nodes numbered k(N+1)^2 + j(N+1) + i, 6 tets per hex (one of them
+ * the zero-volume sliver the reference's split contains). */
+fm_status fm_unit_cube_sizes(int N, uint32_t* n_nodes, uint32_t* n_elems);
+fm_status fm_unit_cube(int N, double* xyz, uint32_t* conn);
+
+/* ---- mesh, pattern, material, boundary conditions (host arrays) ---------
+ * fm_set_mesh replaces the MeshTopology hand-over to the assembly
+ * (FEM/fem_types.hpp:168-211).  elem_volume, if given, is the stored
+ * TetraElement::volume: elements with volume < 1e-30 are skipped exactly as
+ * assemble_global_threadlocal skips them (FEM/adaptive_fem_engine.hpp:1169);
+ * NULL uses |det J|/6 of the given coordinates.  Builds the node neighbour
+ * structure, the solve-pattern CSR and the ILU(0) dependency schedules on
+ * the host and uploads them. */
+fm_status fm_set_mesh(fm_ctx* ctx, uint32_t n_nodes, const double* xyz, uint32_t n_elems,
+                      const uint32_t* conn, const double* elem_volume);
+
+/* Replaces build_csr_sparsity_pattern_rigorous (FEM/adaptive_fem_engine.hpp:1069)
+ * and the element->CSR lookup it feeds (:1141-1150).  Any output may be NULL.
+ * row_ptr_out[n_dofs+1], col_idx_out[nnz], slot_map_out[n_elems*144] with
+ * slot[e][(i*3+di)*12 + j*3+dj] = CSR index of (3n_i+di, 3n_j+dj); for the
+ * reference pattern the last duplicate wins and missing entries are -1. */
+fm_status fm_build_pattern(fm_ctx* ctx, fm_pattern kind, uint32_t* row_ptr_out,
+                           uint32_t* col_idx_out, int32_t* slot_map_out);
+
+/* Material, replaces ProblemDescriptor{E, nu} (FEM/fem_types.hpp:241-256) and
+ * NeoHookeanParameters (FEM/constitutive_models.hpp:30-46).  E_elem (nullable)
+ * gives a per-element Young's modulus with the global nu; mu and lambda are
+ * derived per element as the reference derives them (:81-82). */
+fm_status fm_set_material(fm_ctx* ctx, double E, double nu, const double* E_elem);
+/* Per-element Lame parameters (independent mu_e, lambda_e, as the adjoint's
+ * parameters); nu only enters the tangent's volumetric factor
+ * lambda / (J max(1-2nu, 0.1)) (:170). */
+fm_status fm_set_material_lame(fm_ctx* ctx, const double* mu_elem, const double* lambda_elem,
+                               double nu);
+
+/* Dirichlet data, replaces BoundaryConditions::dirichlet_bcs
+ * (FEM/fem_types.hpp:258-264): dof_mask[n_dofs] (1 = constrained) and the
+ * value at full load (NULL = all zero).  Elimination as in
+ * FEM/nonlinear_solver.hpp:329-334, 388-396: constrained rows/columns of K
+ * are zeroed with a unit diagonal and their residual entries are zero. */
+fm_status fm_set_bc(fm_ctx* ctx, const uint8_t* dof_mask, const double* dof_value_full_load);
+
+/* ---- A5: batched element kernel -------------------------------------------
+ * Replaces tet_element_stiffness_rigorous (FEM/adaptive_fem_engine.hpp:511-701)
+ * for n independent tets: x_dev[12n] (4 nodes xyz), u_dev[12n], E_dev[n];
+ * outputs K_dev[144n] (row-major (i*3+p)*12 + j*3+q) and f_dev[12n]. */
+fm_status fm_elements(fm_ctx* ctx, uint32_t n, const double* x_dev, const double* u_dev,
+                      const double* E_dev, double nu, double* K_dev, double* f_dev);
+
+/* ---- A10/A11/A12: assembly ------------------------------------------------
+ * Replaces assemble_global_threadlocal (FEM/adaptive_fem_engine.hpp:1126-1233)
+ * on the solve pattern.  K_vals_dev: nnz doubles (FM_FP64) or floats
+ * (FM_MIXED), NULL = the context's own buffer (used by fm_ilu0/fm_pcg).
+ * f_int_dev: n_dofs doubles (FP64 in both precisions), may be NULL.
+ * apply_bc != 0 also eliminates the Dirichlet rows/columns in K. */
+fm_status fm_assemble(fm_ctx* ctx, const double* u_dev, void* K_vals_dev, double* f_int_dev,
+                      fm_precision prec, int apply_bc);
+/* Same with host buffers (copies inside the call): the drop-in for callers
+ * holding std::vector data.  K_vals_host: nnz doubles. */
+fm_status fm_assemble_host(fm_ctx* ctx, const double* u_host, double* K_vals_host,
+                           double* f_int_host);
+/* Replaces assemble_global_residual_only (FEM/adaptive_fem_engine.hpp:990-1059). */
+fm_status fm_residual(fm_ctx* ctx, const double* u_dev, double* f_int_dev);
+/* Reference-pattern assembly (the reference's CSR with its fill defect,
+ * last-duplicate-wins slot map), FP64, for structural parity only. */
+fm_status fm_assemble_reference_pattern(fm_ctx* ctx, const double* u_dev, double* K_vals_dev,
+                                        double* f_int_dev);
+
+/* ---- A15: ILU(0) level sets (host arrays) ---------------------------------
+ * True dependency levels of the solve pattern at DOF granularity:
+ * depth_L(i) = 1 + max depth_L(j) over j < i in row i, depth_U likewise
+ * from the bottom; rows of a level ascend.  (The reference's own schedule
+ * is natural order, level[i] = i: FEM/adaptive_fem_engine.hpp:327-349.)
+ * fwd_ptr/bwd_ptr need n_dofs+1 entries of room, *_rows n_dofs. */
+fm_status fm_levels(fm_ctx* ctx, uint32_t* fwd_ptr, uint32_t* fwd_rows, uint32_t* bwd_ptr,
+                    uint32_t* bwd_rows, uint32_t* n_fwd, uint32_t* n_bwd);
+
+/* ---- A13/A14: ILU(0) factorization of the context's K ---------------------
+ * Replaces ILU0Preconditioner::factorize (FEM/adaptive_fem_engine.hpp:305-470);
+ * same values as the reference's natural-order Doolittle elimination with
+ * pivot perturbation (|u_ii| < 1e-12 -> +-1e-8).  Export with fm_get_ilu0. */
+fm_status fm_ilu0(fm_ctx* ctx, fm_precision prec);
+/* Copies out LU (L multipliers on lower slots, U on upper slots, the matrix
+ * value on the diagonal slot as the reference's U_val keeps it) and pivots. */
+fm_status fm_get_ilu0(fm_ctx* ctx, double* LU_host, double* diag_host);
+/* Replaces ILU0Preconditioner::solve (:473-504): y = U^-1 L^-1 r. */
+fm_status fm_ilu0_apply(fm_ctx* ctx, const double* r_dev, double* y_dev);
+
+/* ---- A17/A18: SpMV and PCG on the context's K -----------------------------
+ * fm_spmv replaces SparseCSR::matvec (FEM/fem_types.hpp:310-319).
+ * fm_pcg replaces pcg_solve_ilu0 (FEM/adaptive_fem_engine.hpp:1283-1341) with
+ * the same stop tests; the factorization from fm_ilu0 is reused (call
+ * fm_ilu0 first, as the reference refactors on entry).  *iters = iterations
+ * (max_iter when not converged), *relres = sqrt(r.z / b.b) at exit. */
+fm_status fm_spmv(fm_ctx* ctx, const double* x_dev, double* y_dev);
+fm_status fm_pcg(fm_ctx* ctx, const double* b_dev, double* x_dev, double tol, int max_iter,
+                 int* iters, double* relres, fm_precision prec);
+
+/* ---- generic CSR PCG-ILU(0) (host arrays) ---------------------------------
+ * Drop-in for pcg_solve_ilu0(const SparseCSR&, b, x, N, tol, max_iter)
+ * (FEM/adaptive_fem_engine.hpp:1283) on any square CSR matrix (columns in any
+ * order; ILU works on the sorted pattern as the reference's symbolic phase
+ * does).  x is in/out. */
+fm_status fm_csr_pcg_ilu0(fm_ctx* ctx, uint32_t n, const uint32_t* row_ptr,
+                          const uint32_t* col_idx, const double* val, const double* b, double* x,
+                          double tol, int max_iter, int* iters, double* relres);
+
+/* Drop-in for ILU0Preconditioner::factorize on any CSR (host arrays):
+ * LU_out[nnz] in the caller's column order (L multipliers on lower slots,
+ * U on upper, a_ii kept on the diagonal slot), diag_out[n] the pivots. */
+fm_status fm_csr_ilu0(fm_ctx* ctx, uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx,
+                      const double* val, double* LU_out, double* diag_out);
+
+/* ---- A19/A20: Newton load stepping ----------------------------------------
+ * fm_newton_step: one load level (NonlinearNewtonSolver::solve(u, load, cfg),
+ * FEM/nonlinear_solver.hpp:87): constrained DOFs of u are set to
+ * load_frac * value, then Newton iterations run until
+ * ||R|| < newton_rtol ||R_0|| or ||R|| < newton_atol (R_0: first iteration
+ * of this call).  line_search > 0 enables Armijo backtracking on ||R||
+ * (accept alpha when ||R(u + alpha du)|| <= (1 - ls_c alpha) ||R(u)||,
+ * alpha halved up to line_search times; FEM/adaptive_fem_engine.hpp:933-985
+ * with ls_c = 1e-4, FEM/nonlinear_solver.hpp:156-187 with ls_c = 0.1). */
+fm_status fm_newton_step(fm_ctx* ctx, double* u_dev, double load_frac, double newton_rtol,
+                         double newton_atol, double inner_tol, int max_newton, int max_pcg,
+                         int line_search, double ls_c, fm_precision prec, int* newton_iters,
+                         int* pcg_iters, double* final_relres);
+
+/* fm_newton_solve: load steps first_step..n_load_steps of a load path.
+ * Replaces NonlinearNewtonSolver::solve (FEM/nonlinear_solver.hpp:87-238)
+ * with the engine's mathematics (FEM/adaptive_fem_engine.hpp:2476-2592):
+ * for load step s = 1..n_load_steps the constrained DOFs of u are set to
+ * (s/n) * value; then repeat {assemble, eliminate, R = -f_int,
+ * stop when ||R|| < newton_rtol * ||R at the step's first iteration||
+ * (or < newton_atol), ILU(0), PCG to inner_tol, u += du}.
+ * FM_MIXED: tangent, ILU(0) and PCG in FP32; det F, ln J, f_int, R and u in
+ * FP64 (the Newton loop is the iterative refinement).
+ * newton_iters/pcg_iters (nullable) receive totals over all steps. */
+fm_status fm_newton_solve(fm_ctx* ctx, double* u_dev, int first_step, int n_load_steps,
+                          double newton_rtol, double newton_atol, double inner_tol,
+                          int max_newton, int max_pcg, fm_precision prec, int* newton_iters,
+                          int* pcg_iters, double* final_relres);
+
+/* ---- A9/A21: exact Jacobian and adjoint (no reference counterpart) --------
+ * fm_exact_apply: y = K_exact v (transpose = 0) or K_exact^T v (1), the
+ * derivative of the element forces f_int(u) at u (not the reference's
+ * heuristic tangent), matrix-free.
+ * fm_adjoint: at a converged u solves K_exact^T w = dL/du on the free DOFs
+ * (defect correction preconditioned by the reference tangent's ILU(0)-PCG)
+ * and writes dL/dmu_e = -w_e . df_e/dmu_e and dL/dlambda_e likewise
+ * (L depends on u only; the residual is R = f_ext - f_int).
+ * w_dev (nullable) receives the adjoint vector. */
+fm_status fm_exact_apply(fm_ctx* ctx, const double* u_dev, const double* v_dev, double* y_dev,
+                         int transpose);
+fm_status fm_adjoint(fm_ctx* ctx, const double* u_dev, const double* dLdu_dev,
+                     double* dLdmu_dev, double* dLdlambda_dev, double* w_dev, double tol,
+                     double inner_tol, int max_sweeps, fm_precision prec, int* sweeps,
+                     int* pcg_iters);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FM_API_H */

@@ -501,10 +501,12 @@ int orc_ilu0(uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx, const
             for (uint32_t m = row_ptr[c]; m < row_ptr[c + 1]; ++m) {
                 uint32_t j = col_idx[m];
                 if (j <= c) continue;
+                /* the pivot accumulates U(c,i) even when (i,i) is not in
+                 * row i's pattern (the reference looks U(c,i) up directly) */
+                if (j == i) { u_ii -= l * LU[m]; continue; }
                 int32_t t = pos[j];
                 if (t < 0) continue;
-                if (j == i) u_ii -= l * LU[m];
-                else LU[t] -= l * LU[m];
+                LU[t] -= l * LU[m];
             }
         }
         (void)has_diag;
