@@ -15,6 +15,7 @@
 
 #include "fm_api.h"
 #include "fm_kernels.hpp"
+#include "fm_nodes.hpp"
 #include "fm_setup.hpp"
 
 namespace {
@@ -69,7 +70,7 @@ struct SolverCsr {
 
 template <typename T>
 struct Work {
-    DevBuf<T> K, LU, diag, r, z, p, Ap, t, b, x;
+    DevBuf<T> K, LU, diag, dinv, r, z, p, Ap, t, b, x;
     bool factor_valid = false;
 };
 
@@ -94,6 +95,9 @@ struct fm_ctx {
     DevBuf<uint32_t> nbr_ptr, nbr, inc_ptr, inc_e;
     SolverCsr fem;   // solve pattern of the mesh
     SolverCsr gen;   // generic CSR (fm_csr_pcg_ilu0)
+    // node-block schedule of the solve pattern (ILU(0) and triangular solves)
+    DevBuf<uint32_t> self_pos, node_fwd, node_bwd;
+    uint32_t node_levels_fwd = 0, node_levels_bwd = 0, width_fwd = 0, width_bwd = 0;
     std::vector<uint32_t> lvl_fwd_ptr, lvl_fwd_rows, lvl_bwd_ptr, lvl_bwd_rows;
 
     // material
@@ -120,11 +124,30 @@ struct fm_ctx {
     DevBuf<fm::DevScalars> sc;
     fm::DevScalars* h_sc = nullptr;  // pinned mirror
     DevBuf<double> partials;
-    DevBuf<double> vec_a, vec_b, vec_c;  // FP64 scratch (Newton R, du, trial u)
+    DevBuf<double> vec_a, vec_b, vec_c, vec_d, vec_e;  // FP64 scratch (R, du, trial/f, v, host u)
     int grid_trsv64 = 0, grid_trsv32 = 0;
+
+    // built-in profiler: CUDA events around each launch group on the stream
+    bool prof_on = false;
+    struct ProfRec {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    std::vector<ProfRec> prof_pending;
+    std::vector<cudaEvent_t> prof_pool;
+    double prof_ms[FM_PROF_KINDS] = {};
+    uint64_t prof_calls[FM_PROF_KINDS] = {};
+    uint64_t prof_kernels[FM_PROF_KINDS] = {};
 
     unsigned* status() { return &sc.p->status; }
     unsigned* counter() { return &sc.p->counter[0]; }
+    ~fm_ctx() {
+        for (auto& r : prof_pending) {
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+        for (auto e : prof_pool) cudaEventDestroy(e);
+    }
 };
 
 namespace {
@@ -153,6 +176,52 @@ fm_status fail(fm_ctx* c, fm_status st, const char* fmt, ...) {
         if (s_ != FM_OK) return s_;     \
     } while (0)
 
+// ---- profiler ---------------------------------------------------------------
+cudaEvent_t prof_event(fm_ctx* c) {
+    cudaEvent_t e = nullptr;
+    if (!c->prof_pool.empty()) {
+        e = c->prof_pool.back();
+        c->prof_pool.pop_back();
+    } else if (cudaEventCreate(&e) != cudaSuccess) {
+        e = nullptr;
+    }
+    return e;
+}
+// accumulate completed records (call after the stream was synchronized)
+void prof_flush(fm_ctx* c) {
+    for (auto& r : c->prof_pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) c->prof_ms[r.kind] += ms;
+        c->prof_pool.push_back(r.a);
+        c->prof_pool.push_back(r.b);
+    }
+    c->prof_pending.clear();
+}
+// RAII: records an event pair around the launches of one group of kernels
+struct ProfScope {
+    fm_ctx* c;
+    int kind;
+    cudaEvent_t a = nullptr;
+    ProfScope(fm_ctx* ctx, int k, int kernels) : c(ctx), kind(k) {
+        if (!c->prof_on) return;
+        c->prof_calls[k] += 1;
+        c->prof_kernels[k] += (uint64_t)kernels;
+        a = prof_event(c);
+        if (a) cudaEventRecord(a, c->stream);
+    }
+    ~ProfScope() {
+        if (!a) return;
+        cudaEvent_t b = prof_event(c);
+        if (!b) {
+            c->prof_pool.push_back(a);
+            return;
+        }
+        cudaEventRecord(b, c->stream);
+        c->prof_pending.push_back({kind, a, b});
+    }
+};
+#define PROF(kind, nk) ProfScope prof_scope_(c, kind, nk)
+
 template <typename T>
 cudaError_t upload(DevBuf<T>& d, const T* h, size_t count, cudaStream_t s) {
     cudaError_t e = d.reserve(count ? count : 1);
@@ -165,6 +234,7 @@ fm_status device_flags(fm_ctx* c, uint32_t* flags) {
     CK(cudaMemcpyAsync(c->h_sc, c->sc.p, sizeof(fm::DevScalars), cudaMemcpyDeviceToHost,
                        c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (c->prof_on) prof_flush(c);
     *flags = c->h_sc->status;
     return FM_OK;
 }
@@ -182,6 +252,7 @@ fm_status sync_scalars(fm_ctx* c) {
     CK(cudaMemcpyAsync(c->h_sc, c->sc.p, sizeof(fm::DevScalars), cudaMemcpyDeviceToHost,
                        c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    if (c->prof_on) prof_flush(c);
     return FM_OK;
 }
 
@@ -278,6 +349,19 @@ unsigned next_epoch(fm_ctx* c) {
     return c->epoch;
 }
 
+fm::NodeSched node_sched(const fm_ctx* c) {
+    fm::NodeSched S;
+    S.n_nodes = c->nn;
+    S.nbr_ptr = c->nbr_ptr.p;
+    S.nbr = c->nbr.p;
+    S.self_pos = c->self_pos.p;
+    S.fwd_order = c->node_fwd.p;
+    S.bwd_order = c->node_bwd.p;
+    S.max_width_fwd = c->width_fwd;
+    S.max_width_bwd = c->width_bwd;
+    return S;
+}
+
 // A linear operator for PCG: the mesh K (node-block SpMV) or a generic CSR.
 template <typename T>
 struct Op {
@@ -289,7 +373,9 @@ struct Op {
     const T* diag;
     T* tmp;
     int grid_trsv;
+    const T* dinv = nullptr;  // reciprocal pivots (node-block path)
     void spmv(const T* x, T* y, double* dot) const {
+        PROF(FM_PROF_SPMV, 1);
         T* part = reinterpret_cast<T*>(c->partials.p);
         if (node_block)
             fm::launch_spmv_nodes<T>(c->nn, c->nbr_ptr.p, c->nbr.p, K, x, y, part, c->counter(),
@@ -299,6 +385,12 @@ struct Op {
                                    c->stream);
     }
     void precond(const T* r, T* z) const {
+        PROF(FM_PROF_TRSV, node_block ? 4 : 2);
+        if (node_block) {
+            fm::launch_trsv_nodes<T>(node_sched(c), LU, dinv, r, tmp, z, c->status(), c->device,
+                                     c->stream);
+            return;
+        }
         const fm::CsrDev v = S->view();
         fm::launch_trsv_lower_csr<T>(v, LU, r, tmp, c->done.p, next_epoch(c), c->status(),
                                      grid_trsv, c->stream);
@@ -318,7 +410,7 @@ fm_status pcg_core(fm_ctx* c, const Op<T>& A, uint32_t n, const T* b, T* x, doub
     CK(cudaMemsetAsync(&sc->stop, 0, sizeof(unsigned), c->stream));
     // r = b - A x
     A.spmv(x, w.r.p, nullptr);
-    fm::launch_residual_init<T>(n, b, w.r.p, part, c->counter(), &sc->rr, c->stream);
+    { PROF(FM_PROF_VECTOR, 1); fm::launch_residual_init<T>(n, b, w.r.p, part, c->counter(), &sc->rr, c->stream); }
     TRY(sync_scalars(c));
     TRY(check_flags(c, c->h_sc->status, "pcg"));
     int iters = max_iter;
@@ -327,12 +419,12 @@ fm_status pcg_core(fm_ctx* c, const Op<T>& A, uint32_t n, const T* b, T* x, doub
         iters = 0;
     } else {
         A.precond(w.r.p, w.z.p);
-        fm::launch_pcg_start<T>(n, w.r.p, w.z.p, b, w.p.p, part, c->counter(), sc, c->stream);
+        { PROF(FM_PROF_VECTOR, 1); fm::launch_pcg_start<T>(n, w.r.p, w.z.p, b, w.p.p, part, c->counter(), sc, c->stream); }
         for (int it = 0; it < max_iter; ++it) {
             A.spmv(w.p.p, w.Ap.p, &sc->pAp);
-            fm::launch_pcg_update_xr<T>(n, w.p.p, w.Ap.p, x, w.r.p, sc, c->stream);
+            { PROF(FM_PROF_VECTOR, 1); fm::launch_pcg_update_xr<T>(n, w.p.p, w.Ap.p, x, w.r.p, sc, c->stream); }
             A.precond(w.r.p, w.z.p);
-            fm::launch_pcg_rz<T>(n, w.r.p, w.z.p, part, c->counter(), sc, c->stream);
+            { PROF(FM_PROF_VECTOR, 1); fm::launch_pcg_rz<T>(n, w.r.p, w.z.p, part, c->counter(), sc, c->stream); }
             TRY(sync_scalars(c));
             TRY(check_flags(c, c->h_sc->status, "pcg"));
             if (c->h_sc->stop) break;  // |p.Ap| < 1e-60
@@ -341,7 +433,7 @@ fm_status pcg_core(fm_ctx* c, const Op<T>& A, uint32_t n, const T* b, T* x, doub
                 iters = it + 1;
                 break;
             }
-            fm::launch_pcg_update_p<T>(n, w.z.p, w.p.p, sc, c->stream);
+            { PROF(FM_PROF_VECTOR, 1); fm::launch_pcg_update_p<T>(n, w.z.p, w.p.p, sc, c->stream); }
         }
     }
     if (iters_out) *iters_out = iters;
@@ -351,6 +443,13 @@ fm_status pcg_core(fm_ctx* c, const Op<T>& A, uint32_t n, const T* b, T* x, doub
 
 template <typename T>
 fm_status ilu_core(fm_ctx* c, SolverCsr& S, const T* a, T* lu, T* diag) {
+    PROF(FM_PROF_ILU, 1);
+    if (&S == &c->fem) {
+        fm::launch_ilu0_nodes<T>(node_sched(c), a, lu, diag, work<T>(c).dinv.p, c->done.p,
+                                 next_epoch(c), c->status(), c->device, c->stream);
+        CK(cudaGetLastError());
+        return FM_OK;
+    }
     const fm::CsrDev v = S.view();
     const int grid = fm::persistent_grid_ilu0_csr(c->device, sizeof(T) == 4, v);
     fm::launch_ilu0_csr<T>(v, a, lu, diag, c->done.p, next_epoch(c), c->status(), grid,
@@ -376,6 +475,7 @@ fm_status ensure_matrix(fm_ctx* c) {
     CK(w.K.reserve(c->nnz));
     CK(w.LU.reserve(c->nnz));
     CK(w.diag.reserve(c->n));
+    CK(w.dinv.reserve(c->n));
     return ensure_vectors<T>(c, c->n);
 }
 
@@ -524,6 +624,21 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
         fm::csr_row_ptr(c->graph, rp.data());
         fm::csr_solve_cols(c->graph, ci.data());
         TRY(setup_solver_csr(c, c->fem, c->n, std::move(rp), std::move(ci), true));
+        {
+            std::vector<uint32_t> lp, lo, up, uo;
+            c->node_levels_fwd = fm::node_levels(c->graph, true, lp, lo);
+            c->node_levels_bwd = fm::node_levels(c->graph, false, up, uo);
+            c->width_fwd = c->width_bwd = 0;
+            for (size_t l = 0; l + 1 < lp.size(); ++l)
+                c->width_fwd = std::max(c->width_fwd, lp[l + 1] - lp[l]);
+            for (size_t l = 0; l + 1 < up.size(); ++l)
+                c->width_bwd = std::max(c->width_bwd, up[l + 1] - up[l]);
+            CK(upload(c->self_pos, c->graph.self.data(), c->graph.self.size(), c->stream));
+            CK(upload(c->node_fwd, lo.data(), lo.size(), c->stream));
+            CK(upload(c->node_bwd, uo.data(), uo.size(), c->stream));
+            CK(c->done.reserve(std::max<size_t>(c->done.n, (size_t)c->nn + 1)));
+            CK(cudaMemsetAsync(c->done.p, 0, c->done.n * sizeof(unsigned), c->stream));
+        }
         c->w64.factor_valid = c->w32.factor_valid = false;
         c->has_bc = false;
         c->has_mat = false;
@@ -618,7 +733,7 @@ fm_status fm_set_bc(fm_ctx* c, const uint8_t* dof_mask, const double* dof_value)
 fm_status fm_elements(fm_ctx* c, uint32_t n, const double* x, const double* u, const double* E,
                       double nu, double* K, double* f) {
     if (!c || !x || !u || !E || !K || !f) return fail(c, FM_ERR_ARG, "null argument");
-    fm::launch_elements(n, x, u, E, nu, K, f, c->status(), c->stream);
+    { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_elements(n, x, u, E, nu, K, f, c->status(), c->stream); }
     CK(cudaGetLastError());
     uint32_t flags;
     TRY(device_flags(c, &flags));
@@ -633,12 +748,12 @@ fm_status fm_assemble(fm_ctx* c, const double* u, void* K, double* f, fm_precisi
     if (prec == FM_FP64) {
         TRY(ensure_matrix<double>(c));
         double* Kd = K ? static_cast<double*>(K) : c->w64.K.p;
-        fm::launch_assemble(m, u, Kd, f, nullptr, apply_bc && c->has_bc, c->status(), c->stream);
+        { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble(m, u, Kd, f, nullptr, apply_bc && c->has_bc, c->status(), c->stream); }
         c->w64.factor_valid = false;
     } else if (prec == FM_MIXED) {
         TRY(ensure_matrix<float>(c));
         float* Kf = K ? static_cast<float*>(K) : c->w32.K.p;
-        fm::launch_assemble(m, u, Kf, f, nullptr, apply_bc && c->has_bc, c->status(), c->stream);
+        { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble(m, u, Kf, f, nullptr, apply_bc && c->has_bc, c->status(), c->stream); }
         c->w32.factor_valid = false;
     } else {
         return fail(c, FM_ERR_ARG, "unknown precision");
@@ -654,8 +769,8 @@ fm_status fm_assemble_host(fm_ctx* c, const double* u_host, double* K_host, doub
     CK(cudaMemcpyAsync(c->vec_a.p, u_host, sizeof(double) * c->n, cudaMemcpyHostToDevice,
                        c->stream));
     const fm::MeshDev m = mesh_view(c);
-    fm::launch_assemble(m, c->vec_a.p, c->w64.K.p, c->vec_b.p, nullptr, 0, c->status(),
-                        c->stream);
+    { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble(m, c->vec_a.p, c->w64.K.p, c->vec_b.p, nullptr, 0, c->status(),
+                        c->stream); }
     CK(cudaGetLastError());
     c->w64.factor_valid = false;
     if (K_host)
@@ -673,8 +788,8 @@ fm_status fm_residual(fm_ctx* c, const double* u, double* f) {
     TRY(need_material(c));
     if (!u || !f) return fail(c, FM_ERR_ARG, "null argument");
     const fm::MeshDev m = mesh_view(c);
-    fm::launch_assemble(m, u, static_cast<double*>(nullptr), f, nullptr, 0, c->status(),
-                        c->stream);
+    { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble(m, u, static_cast<double*>(nullptr), f, nullptr, 0, c->status(),
+                        c->stream); }
     CK(cudaGetLastError());
     return FM_OK;
 }
@@ -696,8 +811,8 @@ fm_status fm_assemble_reference_pattern(fm_ctx* c, const double* u, double* K, d
     CK(c->ke_scratch.reserve(144 * (size_t)c->ne));
     CK(cudaMemsetAsync(K, 0, sizeof(double) * c->nnz, c->stream));
     CK(cudaMemsetAsync(f, 0, sizeof(double) * c->n, c->stream));
-    fm::launch_assemble_slotmap(mesh_view(c), u, c->ref_slot.p, K, f, c->ke_scratch.p,
-                                c->status(), c->stream);
+    { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble_slotmap(mesh_view(c), u, c->ref_slot.p, K, f, c->ke_scratch.p,
+                                c->status(), c->stream); }
     CK(cudaGetLastError());
     uint32_t flags;
     TRY(device_flags(c, &flags));
@@ -752,7 +867,7 @@ fm_status fm_ilu0_apply(fm_ctx* c, const double* r, double* y) {
     if (!c->w64.factor_valid) return fail(c, FM_ERR_ARG, "no FP64 factorization: call fm_ilu0");
     if (!r || !y) return fail(c, FM_ERR_ARG, "null argument");
     Op<double> A{c, &c->fem, true, c->w64.K.p, c->w64.LU.p, c->w64.diag.p, c->w64.t.p,
-                 c->grid_trsv64};
+                 c->grid_trsv64, c->w64.dinv.p};
     A.precond(r, y);
     CK(cudaGetLastError());
     uint32_t flags;
@@ -776,13 +891,13 @@ fm_status fm_pcg(fm_ctx* c, const double* b, double* x, double tol, int max_iter
     if (prec == FM_FP64) {
         if (!c->w64.factor_valid) return fail(c, FM_ERR_ARG, "call fm_ilu0(FM_FP64) first");
         Op<double> A{c, &c->fem, true, c->w64.K.p, c->w64.LU.p, c->w64.diag.p, c->w64.t.p,
-                     c->grid_trsv64};
+                     c->grid_trsv64, c->w64.dinv.p};
         return pcg_core<double>(c, A, c->n, b, x, tol, max_iter, iters, relres);
     }
     if (prec != FM_MIXED) return fail(c, FM_ERR_ARG, "unknown precision");
     if (!c->w32.factor_valid) return fail(c, FM_ERR_ARG, "call fm_ilu0(FM_MIXED) first");
     // FP32 inner solve on b/||b||; x returned in FP64
-    fm::launch_norm2(c->n, b, c->partials.p, c->counter(), &c->sc.p->norm2, c->stream);
+    { PROF(FM_PROF_VECTOR, 1); fm::launch_norm2(c->n, b, c->partials.p, c->counter(), &c->sc.p->norm2, c->stream); }
     TRY(sync_scalars(c));
     const double s = std::sqrt(c->h_sc->norm2);
     if (s == 0.0) {
@@ -790,11 +905,11 @@ fm_status fm_pcg(fm_ctx* c, const double* b, double* x, double tol, int max_iter
         if (relres) *relres = 0.0;
         return FM_OK;
     }
-    fm::launch_to_f32_scaled(c->n, b, 1.0 / s, c->w32.b.p, c->w32.x.p, c->stream);
+    { PROF(FM_PROF_VECTOR, 1); fm::launch_to_f32_scaled(c->n, b, 1.0 / s, c->w32.b.p, c->w32.x.p, c->stream); }
     Op<float> A{c, &c->fem, true, c->w32.K.p, c->w32.LU.p, c->w32.diag.p, c->w32.t.p,
-                c->grid_trsv32};
+                c->grid_trsv32, c->w32.dinv.p};
     TRY(pcg_core<float>(c, A, c->n, c->w32.b.p, c->w32.x.p, tol, max_iter, iters, relres));
-    fm::launch_axpy_u_f32(c->n, c->w32.x.p, s, x, c->stream);
+    { PROF(FM_PROF_VECTOR, 1); fm::launch_axpy_u_f32(c->n, c->w32.x.p, s, x, c->stream); }
     CK(cudaGetLastError());
     return FM_OK;
 }
@@ -858,65 +973,115 @@ fm_status fm_newton_step(fm_ctx* c, double* u, double load_frac, double rtol, do
     const bool mixed = prec == FM_MIXED;
     if (mixed) TRY(ensure_matrix<float>(c));
     else TRY(ensure_matrix<double>(c));
-    if (line_search) CK(c->vec_c.reserve(c->n));
+    CK(c->vec_c.reserve(c->n));
+    CK(c->vec_d.reserve(c->n));
     const fm::MeshDev m = mesh_view(c);
     double* R = c->vec_a.p;
     double* du = c->vec_b.p;
-    if (c->has_bc)
-        fm::launch_set_bc_values(c->n, c->mask.p, c->has_bcval ? c->bcval.p : nullptr, load_frac,
-                                 u, c->stream);
     int n_newton = 0, n_pcg = 0;
     double r0 = 0.0, last_rel = 0.0;
-    bool conv = false;
-    for (int it = 0; it < max_newton; ++it) {
+    bool have_r0 = false, conv = false;
+
+    // ILU(0) of the eliminated tangent, PCG on R (norm rn), then either
+    // u += du (no line search) or du kept in `du` (FP64) for the caller.
+    auto solve = [&](double rn, bool keep_du, int* its) -> fm_status {
+        if (mixed) {
+            // FP32 tangent/ILU(0)/PCG on R/||R||; the step is rescaled in FP64
+            TRY(ilu_core<float>(c, c->fem, c->w32.K.p, c->w32.LU.p, c->w32.diag.p));
+            { PROF(FM_PROF_VECTOR, 1); fm::launch_to_f32_scaled(c->n, R, 1.0 / rn, c->w32.b.p, c->w32.x.p, c->stream); }
+            Op<float> A{c, &c->fem, true, c->w32.K.p, c->w32.LU.p, c->w32.diag.p, c->w32.t.p,
+                        c->grid_trsv32, c->w32.dinv.p};
+            TRY(pcg_core<float>(c, A, c->n, c->w32.b.p, c->w32.x.p, inner_tol, max_pcg, its,
+                                nullptr));
+            if (keep_du) { PROF(FM_PROF_VECTOR, 1); fm::launch_f32_to_f64_scaled(c->n, c->w32.x.p, rn, du, c->stream); }
+            else { PROF(FM_PROF_VECTOR, 1); fm::launch_axpy_u_f32(c->n, c->w32.x.p, rn, u, c->stream); }
+        } else {
+            TRY(ilu_core<double>(c, c->fem, c->w64.K.p, c->w64.LU.p, c->w64.diag.p));
+            CK(cudaMemsetAsync(du, 0, sizeof(double) * c->n, c->stream));
+            Op<double> A{c, &c->fem, true, c->w64.K.p, c->w64.LU.p, c->w64.diag.p, c->w64.t.p,
+                         c->grid_trsv64, c->w64.dinv.p};
+            TRY(pcg_core<double>(c, A, c->n, R, du, inner_tol, max_pcg, its, nullptr));
+            if (!keep_du) { PROF(FM_PROF_VECTOR, 1); fm::launch_axpy_u(c->n, du, u, c->stream); }
+        }
+        CK(cudaGetLastError());
+        return FM_OK;
+    };
+
+    if (c->has_bc) {
+        // predictor: spread the prescribed increment v through the body with
+        // the tangent at the current state (K_ff du_f = -f_f - K_fc v_c)
+        double* v = c->vec_d.p;
+        { PROF(FM_PROF_VECTOR, 1); fm::launch_bc_increment(c->n, c->mask.p, c->has_bcval ? c->bcval.p : nullptr, load_frac,
+                                u, v, mixed ? c->w32.b.p : nullptr, c->partials.p, c->counter(),
+                                &c->sc.p->norm2, c->stream); }
+        TRY(sync_scalars(c));
+        if (c->h_sc->norm2 > 0.0 && max_newton > 0) {
+            double* f = c->vec_c.p;
+            if (mixed) {
+                { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble(m, u, c->w32.K.p, f, nullptr, 0, c->status(), c->stream); }
+                { PROF(FM_PROF_SPMV, 1); fm::launch_spmv_nodes<float>(c->nn, c->nbr_ptr.p, c->nbr.p, c->w32.K.p,
+                                             c->w32.b.p, c->w32.Ap.p, nullptr, nullptr, nullptr,
+                                             c->stream); }
+                { PROF(FM_PROF_VECTOR, 1); fm::launch_predictor_rhs<float>(c->n, c->mask.p, f, c->w32.Ap.p, R, c->stream); }
+                { PROF(FM_PROF_VECTOR, 1); fm::launch_apply_bc_nodes<float>(c->nn, c->nbr_ptr.p, c->nbr.p, c->mask.p,
+                                                 c->w32.K.p, c->stream); }
+            } else {
+                { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble(m, u, c->w64.K.p, f, nullptr, 0, c->status(), c->stream); }
+                { PROF(FM_PROF_SPMV, 1); fm::launch_spmv_nodes<double>(c->nn, c->nbr_ptr.p, c->nbr.p, c->w64.K.p, v,
+                                              c->w64.Ap.p, nullptr, nullptr, nullptr, c->stream); }
+                { PROF(FM_PROF_VECTOR, 1); fm::launch_predictor_rhs<double>(c->n, c->mask.p, f, c->w64.Ap.p, R, c->stream); }
+                { PROF(FM_PROF_VECTOR, 1); fm::launch_apply_bc_nodes<double>(c->nn, c->nbr_ptr.p, c->nbr.p, c->mask.p,
+                                                  c->w64.K.p, c->stream); }
+            }
+            { PROF(FM_PROF_VECTOR, 1); fm::launch_norm2(c->n, R, c->partials.p, c->counter(), &c->sc.p->norm2, c->stream); }
+            TRY(sync_scalars(c));
+            TRY(check_flags(c, c->h_sc->status, "newton predictor"));
+            r0 = std::sqrt(c->h_sc->norm2);
+            have_r0 = true;
+            int its = 0;
+            if (r0 > 0.0) TRY(solve(r0, false, &its));
+            n_pcg += its;
+            ++n_newton;
+        }
+        { PROF(FM_PROF_VECTOR, 1); fm::launch_set_bc_values(c->n, c->mask.p, c->has_bcval ? c->bcval.p : nullptr, load_frac,
+                                 u, c->stream); }
+    }
+
+    for (int it = n_newton; it < max_newton; ++it) {
         if (mixed)
-            fm::launch_assemble(m, u, c->w32.K.p, nullptr, R, 1, c->status(), c->stream);
+            { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble(m, u, c->w32.K.p, nullptr, R, 1, c->status(), c->stream); }
         else
-            fm::launch_assemble(m, u, c->w64.K.p, nullptr, R, 1, c->status(), c->stream);
-        fm::launch_norm2(c->n, R, c->partials.p, c->counter(), &c->sc.p->norm2, c->stream);
+            { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble(m, u, c->w64.K.p, nullptr, R, 1, c->status(), c->stream); }
+        { PROF(FM_PROF_VECTOR, 1); fm::launch_norm2(c->n, R, c->partials.p, c->counter(), &c->sc.p->norm2, c->stream); }
         TRY(sync_scalars(c));
         TRY(check_flags(c, c->h_sc->status, "newton assembly"));
         const double rn = std::sqrt(c->h_sc->norm2);
-        if (it == 0) r0 = rn;
+        if (!have_r0) {
+            r0 = rn;
+            have_r0 = true;
+        }
         last_rel = r0 > 0 ? rn / r0 : 0.0;
         if (rn == 0.0 || rn < rtol * r0 || rn < atol) {
             conv = true;
             break;
         }
         int its = 0;
-        if (mixed) {
-            // FP32 tangent/ILU(0)/PCG on R/||R||; the step is rescaled in FP64
-            TRY(ilu_core<float>(c, c->fem, c->w32.K.p, c->w32.LU.p, c->w32.diag.p));
-            fm::launch_to_f32_scaled(c->n, R, 1.0 / rn, c->w32.b.p, c->w32.x.p, c->stream);
-            Op<float> A{c, &c->fem, true, c->w32.K.p, c->w32.LU.p, c->w32.diag.p, c->w32.t.p,
-                        c->grid_trsv32};
-            TRY(pcg_core<float>(c, A, c->n, c->w32.b.p, c->w32.x.p, inner_tol, max_pcg, &its,
-                                nullptr));
-            if (line_search) fm::launch_f32_to_f64_scaled(c->n, c->w32.x.p, rn, du, c->stream);
-            else fm::launch_axpy_u_f32(c->n, c->w32.x.p, rn, u, c->stream);
-        } else {
-            TRY(ilu_core<double>(c, c->fem, c->w64.K.p, c->w64.LU.p, c->w64.diag.p));
-            CK(cudaMemsetAsync(du, 0, sizeof(double) * c->n, c->stream));
-            Op<double> A{c, &c->fem, true, c->w64.K.p, c->w64.LU.p, c->w64.diag.p, c->w64.t.p,
-                         c->grid_trsv64};
-            TRY(pcg_core<double>(c, A, c->n, R, du, inner_tol, max_pcg, &its, nullptr));
-            if (!line_search) fm::launch_axpy_u(c->n, du, u, c->stream);
-        }
+        TRY(solve(rn, line_search > 0, &its));
         if (line_search) {
             // Armijo backtracking on the residual norm with residual-only
             // re-assembly at each trial point
             double alpha = 1.0;
             for (int bt = 0; bt < line_search; ++bt) {
-                fm::launch_trial(c->n, u, alpha, du, c->vec_c.p, c->stream);
-                fm::launch_assemble(m, c->vec_c.p, static_cast<double*>(nullptr), nullptr, R, 0,
-                                    c->status(), c->stream);
-                fm::launch_norm2(c->n, R, c->partials.p, c->counter(), &c->sc.p->norm2,
-                                 c->stream);
+                { PROF(FM_PROF_VECTOR, 1); fm::launch_trial(c->n, u, alpha, du, c->vec_c.p, c->stream); }
+                { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble(m, c->vec_c.p, static_cast<double*>(nullptr), nullptr, R, 0,
+                                    c->status(), c->stream); }
+                { PROF(FM_PROF_VECTOR, 1); fm::launch_norm2(c->n, R, c->partials.p, c->counter(), &c->sc.p->norm2,
+                                 c->stream); }
                 TRY(sync_scalars(c));
                 if (std::sqrt(c->h_sc->norm2) <= (1.0 - ls_c * alpha) * rn) break;
                 if (bt + 1 < line_search) alpha *= 0.5;
             }
-            fm::launch_trial(c->n, u, alpha, du, u, c->stream);
+            { PROF(FM_PROF_VECTOR, 1); fm::launch_trial(c->n, u, alpha, du, u, c->stream); }
         }
         CK(cudaGetLastError());
         n_pcg += its;
@@ -998,6 +1163,49 @@ fm_status fm_csr_ilu0(fm_ctx* c, uint32_t n, const uint32_t* row_ptr, const uint
             for (uint64_t k = 0; k < nnz; ++k) LU_out[perm[k]] = lu[k];
     } catch (const std::bad_alloc&) {
         return fail(c, FM_ERR_OOM, "host allocation failed");
+    }
+    return FM_OK;
+}
+
+fm_status fm_newton_step_host(fm_ctx* c, double* u_host, double load_frac, double rtol,
+                              double atol, double inner_tol, int max_newton, int max_pcg,
+                              int line_search, double ls_c, fm_precision prec, int* newton_iters,
+                              int* pcg_iters, double* final_relres) {
+    TRY(need_mesh(c));
+    if (!u_host) return fail(c, FM_ERR_ARG, "u is null");
+    CK(c->vec_e.reserve(c->n));
+    CK(cudaMemcpyAsync(c->vec_e.p, u_host, sizeof(double) * c->n, cudaMemcpyHostToDevice,
+                       c->stream));
+    fm_status st = fm_newton_step(c, c->vec_e.p, load_frac, rtol, atol, inner_tol, max_newton,
+                                  max_pcg, line_search, ls_c, prec, newton_iters, pcg_iters,
+                                  final_relres);
+    if (st != FM_OK && st != FM_ERR_NOT_CONVERGED) return st;
+    CK(cudaMemcpyAsync(u_host, c->vec_e.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return st;
+}
+
+fm_status fm_profile_enable(fm_ctx* c, int on) {
+    if (!c) return FM_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    prof_flush(c);
+    for (int k = 0; k < FM_PROF_KINDS; ++k) {
+        c->prof_ms[k] = 0.0;
+        c->prof_calls[k] = c->prof_kernels[k] = 0;
+    }
+    c->prof_on = on != 0;
+    return FM_OK;
+}
+
+fm_status fm_profile_read(fm_ctx* c, fm_profile* out) {
+    if (!c || !out) return FM_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    prof_flush(c);
+    for (int k = 0; k < FM_PROF_KINDS; ++k) {
+        out->ms[k] = c->prof_ms[k];
+        out->calls[k] = c->prof_calls[k];
+        out->kernels[k] = c->prof_kernels[k];
     }
     return FM_OK;
 }

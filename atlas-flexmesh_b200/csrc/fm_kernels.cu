@@ -773,7 +773,86 @@ void launch_trial(uint32_t n, const double* u, double alpha, const double* du, d
     k_axpby_trial<<<kRedBlocks * 2, kVecThreads, 0, s>>>(n, u, alpha, du, y);
 }
 
+// Load-step predictor: v = frac*val - u on constrained DOFs (0 elsewhere),
+// in FP64 and (optionally) FP32; ||v||^2 through the deterministic reduction.
+__global__ void __launch_bounds__(kVecThreads)
+    k_bc_increment(uint32_t n, const uint8_t* __restrict__ mask, const double* __restrict__ val,
+                   double frac, const double* __restrict__ u, double* __restrict__ v,
+                   float* __restrict__ v32, double* partials, unsigned* counter, double* out) {
+    double s = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        const double d = mask[i] ? (val ? frac * val[i] : 0.0) - u[i] : 0.0;
+        v[i] = d;
+        if (v32) v32[i] = (float)d;
+        s += d * d;
+    }
+    __shared__ double sbuf[32];
+    const double bt = block_sum(s, sbuf);
+    grid_reduce_finish<double>(bt, partials, counter, [&](double total) { *out = total; });
+}
+void launch_bc_increment(uint32_t n, const uint8_t* mask, const double* val, double frac,
+                         const double* u, double* v, float* v32, double* partials,
+                         unsigned* counter, double* out, cudaStream_t s) {
+    k_bc_increment<<<kRedBlocks, kVecThreads, 0, s>>>(n, mask, val, frac, u, v, v32, partials,
+                                                     counter, out);
+}
+
+// R = -f - K v on free DOFs, 0 on constrained
+template <typename T>
+__global__ void k_predictor_rhs(uint32_t n, const uint8_t* __restrict__ mask,
+                                const double* __restrict__ f, const T* __restrict__ Kv,
+                                double* __restrict__ R) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        R[i] = mask[i] ? 0.0 : -f[i] - (double)Kv[i];
+}
+template <typename T>
+void launch_predictor_rhs(uint32_t n, const uint8_t* mask, const double* f, const T* Kv,
+                          double* R, cudaStream_t s) {
+    k_predictor_rhs<T><<<kRedBlocks * 2, kVecThreads, 0, s>>>(n, mask, f, Kv, R);
+}
+
+// Dirichlet elimination on an assembled node-block K: entries in a
+// constrained row or column become 0, constrained diagonals 1.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_apply_bc_nodes(uint32_t nn, const uint32_t* __restrict__ nbr_ptr,
+                     const uint32_t* __restrict__ nbr, const uint8_t* __restrict__ mask,
+                     T* __restrict__ K) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t n = warp; n < nn; n += nwarps) {
+        const uint32_t nb0 = nbr_ptr[n];
+        const int deg = (int)(nbr_ptr[n + 1] - nb0);
+        const int rl = 3 * deg;
+        T* v = K + 9 * (size_t)nb0;
+        for (int idx = lane; idx < 3 * rl; idx += 32) {
+            const int p = idx / rl;
+            const int rem = idx - p * rl;
+            const int k = rem / 3;
+            const uint32_t row = 3 * n + p;
+            const uint32_t col = 3 * __ldg(nbr + nb0 + k) + (rem - 3 * k);
+            if (mask[row] | mask[col]) v[idx] = (row == col) ? T(1) : T(0);
+        }
+    }
+}
+template <typename T>
+void launch_apply_bc_nodes(uint32_t nn, const uint32_t* nbr_ptr, const uint32_t* nbr,
+                           const uint8_t* mask, T* K, cudaStream_t s) {
+    k_apply_bc_nodes<T><<<kSpmvBlocks, 256, 0, s>>>(nn, nbr_ptr, nbr, mask, K);
+}
+
 // ---- explicit instantiations ------------------------------------------------
+template void launch_predictor_rhs<double>(uint32_t, const uint8_t*, const double*,
+                                           const double*, double*, cudaStream_t);
+template void launch_predictor_rhs<float>(uint32_t, const uint8_t*, const double*, const float*,
+                                          double*, cudaStream_t);
+template void launch_apply_bc_nodes<double>(uint32_t, const uint32_t*, const uint32_t*,
+                                            const uint8_t*, double*, cudaStream_t);
+template void launch_apply_bc_nodes<float>(uint32_t, const uint32_t*, const uint32_t*,
+                                           const uint8_t*, float*, cudaStream_t);
 #define FM_INST(T)                                                                              \
     template void launch_spmv_nodes<T>(uint32_t, const uint32_t*, const uint32_t*, const T*,    \
                                        const T*, T*, T*, unsigned*, double*, cudaStream_t);     \

@@ -117,6 +117,16 @@ void launch_to_f32_scaled(uint32_t n, const double* R, double inv_scale, float* 
 void launch_axpy_u(uint32_t n, const double* du, double* u, cudaStream_t s);
 // u += scale * du32
 void launch_axpy_u_f32(uint32_t n, const float* du, double scale, double* u, cudaStream_t s);
+// load-step predictor pieces
+void launch_bc_increment(uint32_t n, const uint8_t* mask, const double* val, double frac,
+                         const double* u, double* v, float* v32, double* partials,
+                         unsigned* counter, double* out, cudaStream_t s);
+template <typename T>
+void launch_predictor_rhs(uint32_t n, const uint8_t* mask, const double* f, const T* Kv,
+                          double* R, cudaStream_t s);
+template <typename T>
+void launch_apply_bc_nodes(uint32_t nn, const uint32_t* nbr_ptr, const uint32_t* nbr,
+                           const uint8_t* mask, T* K, cudaStream_t s);
 // y = scale * x (FP32 -> FP64)
 void launch_f32_to_f64_scaled(uint32_t n, const float* x, double scale, double* y,
                               cudaStream_t s);

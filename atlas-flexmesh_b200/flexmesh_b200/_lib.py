@@ -28,8 +28,14 @@ EXPORTS = [
     "fm_set_material_lame", "fm_set_bc", "fm_elements", "fm_assemble", "fm_assemble_host",
     "fm_residual", "fm_assemble_reference_pattern", "fm_levels", "fm_ilu0", "fm_get_ilu0",
     "fm_ilu0_apply", "fm_spmv", "fm_pcg", "fm_csr_pcg_ilu0", "fm_newton_solve",
-    "fm_exact_apply", "fm_adjoint", "fm_csr_ilu0", "fm_newton_step",
+    "fm_exact_apply", "fm_adjoint", "fm_csr_ilu0", "fm_newton_step", "fm_newton_step_host",
+    "fm_profile_enable", "fm_profile_read",
 ]
+PROF_KINDS = {0: "assemble", 1: "ilu0", 2: "trsv", 3: "spmv", 4: "vector"}
+
+
+class Profile(C.Structure):
+    _fields_ = [("ms", C.c_double * 8), ("calls", C.c_uint64 * 8), ("kernels", C.c_uint64 * 8)]
 
 
 class FMError(RuntimeError):
@@ -82,6 +88,10 @@ def lib() -> C.CDLL:
             "fm_csr_ilu0": [_vp, _u32, _vp, _vp, _vp, _vp, _vp],
             "fm_newton_step": [_vp, _vp, _f64, _f64, _f64, _f64, _i32, _i32, _i32, _f64, _i32,
                                _P(_i32), _P(_i32), _P(_f64)],
+            "fm_newton_step_host": [_vp, _vp, _f64, _f64, _f64, _f64, _i32, _i32, _i32, _f64,
+                                    _i32, _P(_i32), _P(_i32), _P(_f64)],
+            "fm_profile_enable": [_vp, _i32],
+            "fm_profile_read": [_vp, _P(Profile)],
             "fm_exact_apply": [_vp, _vp, _vp, _vp, _i32],
             "fm_adjoint": [_vp, _vp, _vp, _vp, _vp, _vp, _f64, _f64, _i32, _i32, _P(_i32),
                            _P(_i32)],
@@ -131,9 +141,15 @@ class Context:
         self.torch = torch
         self.device = device
         self._h = _vp()
-        s = None
-        if stream is not None:
-            s = _vp(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        # default: torch's current stream, so library work is ordered with the
+        # torch copies/kernels that produce inputs and read results
+        if stream is None:
+            stream = torch.cuda.current_stream(device)
+        h = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        # handle 0 is the legacy default stream; NULL would ask the library
+        # for a private stream, so pass cudaStreamLegacy (0x1) instead
+        s = _vp(h if h else 1)
+        self.stream = stream
         self._check(lib().fm_create(C.byref(self._h), device, s), "fm_create")
         self.n_nodes = self.n_elems = self.n_dofs = self.nnz = 0
 
@@ -328,6 +344,29 @@ class Context:
             self._check(st, "fm_newton_step")
         return {"newton_iters": nit.value, "pcg_iters": pit.value, "final_relres": rel.value,
                 "status": st}
+
+    def newton_step_host(self, u_host, load_frac, rtol=1e-10, atol=0.0, inner_tol=1e-12,
+                         max_newton=200, max_pcg=5000, line_search=0, ls_c=0.1, prec=FM_FP64,
+                         allow_not_converged=False):
+        """u_host: contiguous float64 numpy array, updated in place"""
+        assert u_host.dtype == np.float64 and u_host.flags.c_contiguous
+        nit, pit, rel = _i32(), _i32(), _f64()
+        st = lib().fm_newton_step_host(self._h, _hp(u_host), load_frac, rtol, atol, inner_tol,
+                                       max_newton, max_pcg, line_search, ls_c, prec,
+                                       C.byref(nit), C.byref(pit), C.byref(rel))
+        if st and not (allow_not_converged and st == 8):
+            self._check(st, "fm_newton_step_host")
+        return {"newton_iters": nit.value, "pcg_iters": pit.value, "final_relres": rel.value,
+                "status": st}
+
+    def profile_enable(self, on=True):
+        self._check(lib().fm_profile_enable(self._h, int(on)), "fm_profile_enable")
+
+    def profile_read(self):
+        p = Profile()
+        self._check(lib().fm_profile_read(self._h, C.byref(p)), "fm_profile_read")
+        return {name: {"ms": p.ms[k], "calls": p.calls[k], "kernels": p.kernels[k]}
+                for k, name in PROF_KINDS.items()}
 
     def exact_apply(self, u, v, transpose=False):
         y = self._zeros(self.n_dofs)

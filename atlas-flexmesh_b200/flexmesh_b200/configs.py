@@ -42,6 +42,10 @@ class Problem:
     E_elem: np.ndarray | None = None   # per-element Young's modulus (None: uniform E)
     mask: np.ndarray = field(default=None)
     bc_value: np.ndarray = field(default=None)
+    # the mesh generator's stored TetraElement::volume (computed before any
+    # jitter, as generate_unit_cube_mesh stores it); the assembly skips
+    # elements whose stored volume is < 1e-30, i.e. the slivers of the split
+    elem_volume: np.ndarray | None = None
     n_steps: int = 1
     meta: dict = field(default_factory=dict)
 
@@ -60,6 +64,18 @@ class Problem:
         mu = E / (2.0 * (1.0 + nu))
         lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
         return mu, lam
+
+
+def tet_volumes(xyz, conn):
+    """|triple product| / 6 per tet (tet_volume, FEM/mesh_adaptation.hpp:111-126)"""
+    X = xyz.reshape(-1, 3)
+    c = conn.reshape(-1, 4)
+    a, b, cc, d = X[c[:, 0]], X[c[:, 1]], X[c[:, 2]], X[c[:, 3]]
+    u, v, w = b - a, cc - a, d - a
+    s6 = (u[:, 0] * (v[:, 1] * w[:, 2] - v[:, 2] * w[:, 1])
+          - u[:, 1] * (v[:, 0] * w[:, 2] - v[:, 2] * w[:, 0])
+          + u[:, 2] * (v[:, 0] * w[:, 1] - v[:, 1] * w[:, 0]))
+    return np.abs(s6) / 6.0
 
 
 def jitter_interior(xyz, N, amp, seed):
@@ -105,12 +121,13 @@ def top_face_xy_dofs(xyz):
 def unit_cube_problem(name, N, *, jitter=0.0, seed_jitter=SEED_JITTER, sigma_log=0.0,
                       seed_mat=SEED_MAT, nu=0.3, E=1.0, uz_total=-0.1, n_steps=5):
     xyz, conn = unit_cube(N)
+    vol = tet_volumes(xyz, conn)
     if jitter:
         xyz = jitter_interior(xyz, N, jitter, seed_jitter)
     E_elem = lognormal_E(conn.size // 4, sigma_log, seed_mat, nu, E) if sigma_log else None
     mask, val = clamp_top_bc(xyz, uz_total)
     return Problem(name=name, N=N, xyz=xyz, conn=conn, nu=nu, E=E, E_elem=E_elem, mask=mask,
-                   bc_value=val, n_steps=n_steps,
+                   bc_value=val, n_steps=n_steps, elem_volume=vol,
                    meta={"jitter": jitter, "sigma_log": sigma_log, "uz_total": uz_total})
 
 

@@ -68,6 +68,21 @@ enum {
     FM_FLAG_BREAKDOWN = 1u << 5  /* PCG |p.Ap| < 1e-60 */
 };
 
+/* Kernel classes of the built-in profiler. */
+enum {
+    FM_PROF_ASSEMBLE = 0, /* element evaluation + CSR scatter (incl. residual-only) */
+    FM_PROF_ILU = 1,      /* ILU(0) factorization */
+    FM_PROF_TRSV = 2,     /* preconditioner apply: forward + backward solve */
+    FM_PROF_SPMV = 3,     /* K x */
+    FM_PROF_VECTOR = 4,   /* PCG/Newton vector updates and reductions */
+    FM_PROF_KINDS = 8
+};
+typedef struct {
+    double ms[FM_PROF_KINDS];       /* device time per class (CUDA events, ms) */
+    uint64_t calls[FM_PROF_KINDS];  /* launch groups per class */
+    uint64_t kernels[FM_PROF_KINDS];/* kernel launches per class */
+} fm_profile;
+
 /* ---- context ----------------------------------------------------------- */
 /* cuda_stream: a cudaStream_t, or NULL to let the context create its own. */
 fm_status fm_create(fm_ctx** ctx, int device, void* cuda_stream);
@@ -79,6 +94,13 @@ fm_status fm_clear_flags(fm_ctx* ctx);
 /* Size queries after fm_set_mesh: DOFs, CSR nonzeros, node neighbours. */
 fm_status fm_sizes(const fm_ctx* ctx, uint32_t* n_nodes, uint32_t* n_elems, uint32_t* n_dofs,
                    uint64_t* nnz);
+/* Built-in profiler (no reference counterpart; the reference times whole
+ * phases with wall clocks, FEM/adaptive_fem_engine.hpp:1251-1273).
+ * fm_profile_enable(ctx, 1) zeroes the counters and records a CUDA event
+ * pair around every kernel group launched afterwards; fm_profile_read
+ * synchronizes the stream and returns the totals. */
+fm_status fm_profile_enable(fm_ctx* ctx, int on);
+fm_status fm_profile_read(fm_ctx* ctx, fm_profile* out);
 
 /* ---- A1: unit-cube generator (host only) ---------------------------------
  * Replaces generate_unit_cube_mesh, FEM/adaptive_fem_engine.hpp:2219-2294:
@@ -208,6 +230,15 @@ fm_status fm_newton_step(fm_ctx* ctx, double* u_dev, double load_frac, double ne
                          double newton_atol, double inner_tol, int max_newton, int max_pcg,
                          int line_search, double ls_c, fm_precision prec, int* newton_iters,
                          int* pcg_iters, double* final_relres);
+
+/* Host-buffer form of fm_newton_step: u_host (n_dofs doubles, in/out) is
+ * copied to the device, solved and copied back inside the call - the shape
+ * of NonlinearNewtonSolver::solve(Solution& u, ...) whose Solution is a
+ * host std::vector<double>. */
+fm_status fm_newton_step_host(fm_ctx* ctx, double* u_host, double load_frac, double newton_rtol,
+                              double newton_atol, double inner_tol, int max_newton, int max_pcg,
+                              int line_search, double ls_c, fm_precision prec, int* newton_iters,
+                              int* pcg_iters, double* final_relres);
 
 /* fm_newton_solve: load steps first_step..n_load_steps of a load path.
  * Replaces NonlinearNewtonSolver::solve (FEM/nonlinear_solver.hpp:87-238)

@@ -662,12 +662,23 @@ done:
 }
 
 /* ------------------------------------------------------------------ */
-/* A19: Newton with Dirichlet elimination and load stepping           */
-/* (contract: load fraction s/S on the prescribed values at step start,*/
-/* R = -f_int, R = 0 and K row/col eliminated on constrained DOFs,     */
-/* stop when ||R|| < rtol * ||R at the step's first iteration||,       */
-/* du from PCG-ILU(0) to inner_tol, full step u += du).                */
-/* Records per-step Newton and PCG counts when the arrays are given.   */
+/* A19: Newton with Dirichlet elimination and load stepping            */
+/* Contract (the reference's Newton, FEM/adaptive_fem_engine.hpp:2476-  */
+/* 2592, with elimination BCs as FEM/nonlinear_solver.hpp:329-334,     */
+/* 388-396, driven by prescribed displacements):                       */
+/*  load step s, level f = s/S, prescribed increment v = f*val - u on  */
+/*  the constrained DOFs (0 elsewhere):                                */
+/*  predictor (when v != 0): K, f_int at u without elimination;        */
+/*    R = -f_int - K v on free DOFs, 0 on constrained; r0 = ||R||;     */
+/*    eliminate; du = PCG(K, R); u_free += du; u_c = f*val.            */
+/*  Newton: assemble, eliminate, R = -f_int (0 on constrained);        */
+/*    stop when ||R|| < rtol * r0 (r0 = first ||R|| if no predictor);  */
+/*    du = PCG-ILU(0)(K, R) to inner_tol; u += du.                     */
+/* The predictor spreads the boundary increment through the body       */
+/* (a linearized lifting); without it a full increment on the top face */
+/* puts a strain of u_z/h into the top element layer and the Newton    */
+/* iteration with the reference's tangent diverges on fine meshes.    */
+/* Newton counts include the predictor solve.                          */
 /* Returns 0 on convergence of every step, 1 otherwise.                */
 /* ------------------------------------------------------------------ */
 int orc_newton(uint32_t n_nodes, uint32_t n_elems, const double* xyz, const uint32_t* conn,
@@ -682,21 +693,38 @@ int orc_newton(uint32_t n_nodes, uint32_t n_elems, const double* xyz, const uint
     double* f = (double*)malloc(sizeof(double) * n);
     double* R = (double*)malloc(sizeof(double) * n);
     double* du = (double*)malloc(sizeof(double) * n);
+    double* v = (double*)malloc(sizeof(double) * n);
     int status = 0;
     for (int s = 1; s <= n_steps; ++s) {
         double frac = (double)s / (double)n_steps;
-        for (uint32_t i = 0; i < n; ++i)
-            if (mask[i]) u[i] = frac * bc_value[i];
         double r0 = 0.0;
-        int it, pcg_total = 0, conv = 0;
-        for (it = 0; it < max_newton; ++it) {
+        int it = 0, pcg_total = 0, conv = 0, have_r0 = 0;
+        int any = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            v[i] = mask[i] ? frac * bc_value[i] - u[i] : 0.0;
+            if (v[i] != 0.0) any = 1;
+        }
+        if (any) {
+            orc_assemble(n_nodes, n_elems, xyz, conn, active, mu_e, lam_e, nu, u, slot, nnz, K, f);
+            orc_spmv(n, row_ptr, col_idx, K, v, R);
+            for (uint32_t i = 0; i < n; ++i) R[i] = mask[i] ? 0.0 : -f[i] - R[i];
+            orc_apply_bc(n, row_ptr, col_idx, K, NULL, mask);
+            for (uint32_t i = 0; i < n; ++i) r0 += R[i] * R[i];
+            r0 = sqrt(r0);
+            have_r0 = 1;
+            memset(du, 0, sizeof(double) * n);
+            pcg_total += orc_pcg_ilu0(n, row_ptr, col_idx, K, R, du, inner_tol, max_pcg, NULL);
+            for (uint32_t i = 0; i < n; ++i) u[i] = mask[i] ? frac * bc_value[i] : u[i] + du[i];
+            it = 1;
+        }
+        for (; it < max_newton; ++it) {
             orc_assemble(n_nodes, n_elems, xyz, conn, active, mu_e, lam_e, nu, u, slot, nnz, K, f);
             for (uint32_t i = 0; i < n; ++i) R[i] = -f[i];
             orc_apply_bc(n, row_ptr, col_idx, K, R, mask);
             double rn = 0.0;
             for (uint32_t i = 0; i < n; ++i) rn += R[i] * R[i];
             rn = sqrt(rn);
-            if (it == 0) r0 = rn;
+            if (!have_r0) { r0 = rn; have_r0 = 1; }
             if (rn == 0.0 || rn < rtol * r0) { conv = 1; break; }
             memset(du, 0, sizeof(double) * n);
             pcg_total += orc_pcg_ilu0(n, row_ptr, col_idx, K, R, du, inner_tol, max_pcg, NULL);
@@ -706,7 +734,7 @@ int orc_newton(uint32_t n_nodes, uint32_t n_elems, const double* xyz, const uint
         if (newton_per_step) newton_per_step[s - 1] = it;
         if (pcg_per_step) pcg_per_step[s - 1] = pcg_total;
     }
-    free(K); free(f); free(R); free(du);
+    free(K); free(f); free(R); free(du); free(v);
     return status;
 }
 

@@ -13,7 +13,10 @@ import oracle as O
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
-TOL_ELEM = 1e-13   # element K/f, normwise max-relative
+# element K/f on random, poorly shaped tets, normwise max-relative: the
+# kernel evaluates the Mandel stress as mu (C - I) + lam lnJ I, the reference
+# as C S with C^-1, whose own rounding grows with cond(C)
+TOL_ELEM = 1e-12
 TOL_ASM = 1e-13    # assembled K.val / f_int, normwise max-relative
 TOL_ILU = 1e-12    # L, U multipliers and pivots, normwise max-relative
 TOL_U = 1e-10      # Newton displacement vs oracle, relative 2-norm
