@@ -97,6 +97,7 @@ struct fm_ctx {
     SolverCsr gen;   // generic CSR (fm_csr_pcg_ilu0)
     // node-block schedule of the solve pattern (ILU(0) and triangular solves)
     DevBuf<uint32_t> self_pos, node_fwd, node_bwd;
+    DevBuf<uint4> node_fwd_rec, node_bwd_rec;
     uint32_t node_levels_fwd = 0, node_levels_bwd = 0, width_fwd = 0, width_bwd = 0;
     std::vector<uint32_t> lvl_fwd_ptr, lvl_fwd_rows, lvl_bwd_ptr, lvl_bwd_rows;
 
@@ -357,6 +358,8 @@ fm::NodeSched node_sched(const fm_ctx* c) {
     S.self_pos = c->self_pos.p;
     S.fwd_order = c->node_fwd.p;
     S.bwd_order = c->node_bwd.p;
+    S.fwd_rec = c->node_fwd_rec.p;
+    S.bwd_rec = c->node_bwd_rec.p;
     S.max_width_fwd = c->width_fwd;
     S.max_width_bwd = c->width_bwd;
     return S;
@@ -636,6 +639,20 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
             CK(upload(c->self_pos, c->graph.self.data(), c->graph.self.size(), c->stream));
             CK(upload(c->node_fwd, lo.data(), lo.size(), c->stream));
             CK(upload(c->node_bwd, uo.data(), uo.size(), c->stream));
+            // one 16-byte schedule record per position of each order
+            auto records = [&](const std::vector<uint32_t>& ord) {
+                std::vector<uint4> rec(ord.size());
+                for (size_t t = 0; t < ord.size(); ++t) {
+                    const uint32_t nd = ord[t];
+                    rec[t] = make_uint4(nd, c->graph.ptr[nd], c->graph.ptr[nd + 1] - c->graph.ptr[nd],
+                                        c->graph.self[nd]);
+                }
+                return rec;
+            };
+            const std::vector<uint4> rf = records(lo), rb = records(uo);
+            CK(upload(c->node_fwd_rec, rf.data(), rf.size(), c->stream));
+            CK(upload(c->node_bwd_rec, rb.data(), rb.size(), c->stream));
+            CK(cudaStreamSynchronize(c->stream));
             CK(c->done.reserve(std::max<size_t>(c->done.n, (size_t)c->nn + 1)));
             CK(cudaMemsetAsync(c->done.p, 0, c->done.n * sizeof(unsigned), c->stream));
         }

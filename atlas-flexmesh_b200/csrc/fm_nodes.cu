@@ -10,212 +10,21 @@
 // Scheduling is sync-free: a persistent grid walks nodes in a topological
 // order (dependency levels); every warp handles positions w, w+W, ... of
 // that order, so the lowest unfinished node always has its inputs complete
-// and all waits end.  Triangular solves wait on the dependency's VALUES: the
-// output vector is pre-filled with a NaN sentinel that arithmetic cannot
-// produce, and a consumer spins (bounded) until the three values of a
-// neighbour are no longer the sentinel - one L2 round trip per dependency.
-// The factorization, whose outputs are whole rows, releases a per-node flag.
+// and all waits end.  The factorization, whose outputs are whole rows,
+// releases a per-node flag; the triangular solves (fm_trsv.cu) wait on the
+// dependencies' values directly.
 #include "fm_kernels.hpp"
 #include "fm_nodes.hpp"
+#include "fm_sync.cuh"
 
 namespace fm {
 
 constexpr int kNodeWarps = 8;
 
 template <typename T>
-struct Sentinel;
-template <>
-struct Sentinel<double> {
-    static __device__ __forceinline__ double value() {
-        return __longlong_as_double(0x7ff4dead0000beefll);
-    }
-    static __device__ __forceinline__ bool is(double v) {
-        return __double_as_longlong(v) == 0x7ff4dead0000beefll;
-    }
-};
-template <>
-struct Sentinel<float> {
-    static __device__ __forceinline__ float value() { return __int_as_float(0x7fa0beef); }
-    static __device__ __forceinline__ bool is(float v) { return __float_as_int(v) == 0x7fa0beef; }
-};
-
-__device__ __forceinline__ double ld_relaxed(const double* p) {
-    double v;
-    asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ float ld_relaxed(const float* p) {
-    float v;
-    asm volatile("ld.relaxed.gpu.global.f32 %0, [%1];" : "=f"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_relaxed(double* p, double v) {
-    asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
-}
-__device__ __forceinline__ void st_relaxed(float* p, float v) {
-    asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
-}
-
-// Spin (bounded) until *p is not the sentinel; returns the value, or the
-// sentinel when the wait gave up (FM_FLAG_TIMEOUT then set).
-template <typename T>
-__device__ __forceinline__ T wait_value(const T* p, unsigned* status) {
-    T v = ld_relaxed(p);
-    if (!Sentinel<T>::is(v)) return v;
-    const long long t0 = clock64();
-    for (unsigned it = 1;; ++it) {
-        v = ld_relaxed(p);
-        if (!Sentinel<T>::is(v)) return v;
-        if ((it & 63u) == 0) {
-            if (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) return v;
-            if (clock64() - t0 > kWaitCycles) {
-                raise_flag(status, FM_FLAG_TIMEOUT);
-                return v;
-            }
-        }
-    }
-}
-
-template <typename T>
 __global__ void k_fill_sentinel(uint32_t n, T* __restrict__ x) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         x[i] = Sentinel<T>::value();
-}
-
-// ---------------------------------------------------------------------------
-// Forward solve L z = r (L unit lower), one warp per node, value-sentinel waits.
-// Every lane owns up to 3 (neighbour, column) items; everything that does not
-// depend on the neighbours' values (indices, LU entries, r, the node's own
-// block) is loaded before the first wait, so a dependency costs one poll.
-// ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(kNodeWarps * 32)
-    k_trsv_lower_nodes(NodeSched S, const T* __restrict__ lu, const T* __restrict__ r,
-                       T* __restrict__ z, unsigned* __restrict__ status) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t W = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t t = gw; t < S.n_nodes; t += W) {
-        const uint32_t n = __ldg(S.fwd_order + t);
-        const uint32_t nb0 = __ldg(S.nbr_ptr + n);
-        const int deg = (int)(__ldg(S.nbr_ptr + n + 1) - nb0);
-        const int sk = (int)__ldg(S.self_pos + n);  // lower neighbours are k < sk
-        const T* row = lu + 9 * (size_t)nb0;
-        const int rl = 3 * deg, ni = 3 * sk;
-        T a0[3], a1[3], a2[3];
-        const T* zp[3];
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const int idx = lane + 32 * j;
-            zp[j] = nullptr;
-            a0[j] = a1[j] = a2[j] = T(0);
-            if (idx < ni) {
-                const int k = idx / 3;
-                zp[j] = z + 3 * (size_t)__ldg(S.nbr + nb0 + k) + (idx - 3 * k);
-                a0[j] = __ldg(row + idx);
-                a1[j] = __ldg(row + rl + idx);
-                a2[j] = __ldg(row + 2 * rl + idx);
-            }
-        }
-        T r0 = T(0), r1 = T(0), r2 = T(0), l10 = T(0), l20 = T(0), l21 = T(0);
-        if (lane == 0) {
-            r0 = __ldg(r + 3 * (size_t)n);
-            r1 = __ldg(r + 3 * (size_t)n + 1);
-            r2 = __ldg(r + 3 * (size_t)n + 2);
-            l10 = __ldg(row + rl + ni);
-            l20 = __ldg(row + 2 * rl + ni);
-            l21 = __ldg(row + 2 * rl + ni + 1);
-        }
-        T s0 = T(0), s1 = T(0), s2 = T(0);
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-            if (zp[j]) {
-                const T zv = wait_value(zp[j], status);
-                s0 += a0[j] * zv;
-                s1 += a1[j] * zv;
-                s2 += a2[j] * zv;
-            }
-        s0 = warp_sum(s0);
-        s1 = warp_sum(s1);
-        s2 = warp_sum(s2);
-        if (lane == 0) {
-            const T z0 = r0 - s0;
-            const T z1 = r1 - s1 - l10 * z0;
-            const T z2 = r2 - s2 - l20 * z0 - l21 * z1;
-            st_relaxed(z + 3 * (size_t)n, z0);
-            st_relaxed(z + 3 * (size_t)n + 1, z1);
-            st_relaxed(z + 3 * (size_t)n + 2, z2);
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Backward solve U y = z with reciprocal pivots dinv, reverse topological order
-// ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(kNodeWarps * 32)
-    k_trsv_upper_nodes(NodeSched S, const T* __restrict__ lu, const T* __restrict__ dinv,
-                       const T* __restrict__ z, T* __restrict__ y, unsigned* __restrict__ status) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t W = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t t = gw; t < S.n_nodes; t += W) {
-        const uint32_t n = __ldg(S.bwd_order + t);
-        const uint32_t nb0 = __ldg(S.nbr_ptr + n);
-        const int deg = (int)(__ldg(S.nbr_ptr + n + 1) - nb0);
-        const int sk = (int)__ldg(S.self_pos + n);  // upper neighbours are k > sk
-        const T* row = lu + 9 * (size_t)nb0;
-        const int rl = 3 * deg, lo = 3 * (sk + 1), ds = 3 * sk;
-        T a0[3], a1[3], a2[3];
-        const T* yp[3];
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const int idx = lo + lane + 32 * j;
-            yp[j] = nullptr;
-            a0[j] = a1[j] = a2[j] = T(0);
-            if (idx < rl) {
-                const int k = idx / 3;
-                yp[j] = y + 3 * (size_t)__ldg(S.nbr + nb0 + k) + (idx - 3 * k);
-                a0[j] = __ldg(row + idx);
-                a1[j] = __ldg(row + rl + idx);
-                a2[j] = __ldg(row + 2 * rl + idx);
-            }
-        }
-        const size_t b = 3 * (size_t)n;
-        T z0 = T(0), z1 = T(0), z2 = T(0), u01 = T(0), u02 = T(0), u12 = T(0);
-        T i0 = T(0), i1 = T(0), i2 = T(0);
-        if (lane == 0) {
-            z0 = z[b];
-            z1 = z[b + 1];
-            z2 = z[b + 2];
-            u01 = __ldg(row + ds + 1);
-            u02 = __ldg(row + ds + 2);
-            u12 = __ldg(row + rl + ds + 2);
-            i0 = __ldg(dinv + b);
-            i1 = __ldg(dinv + b + 1);
-            i2 = __ldg(dinv + b + 2);
-        }
-        T s0 = T(0), s1 = T(0), s2 = T(0);
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-            if (yp[j]) {
-                const T yv = wait_value(yp[j], status);
-                s0 += a0[j] * yv;
-                s1 += a1[j] * yv;
-                s2 += a2[j] * yv;
-            }
-        s0 = warp_sum(s0);
-        s1 = warp_sum(s1);
-        s2 = warp_sum(s2);
-        if (lane == 0) {
-            const T y2 = (z2 - s2) * i2;
-            const T y1 = (z1 - s1 - u12 * y2) * i1;
-            const T y0 = (z0 - s0 - u01 * y1 - u02 * y2) * i0;
-            st_relaxed(y + b, y0);
-            st_relaxed(y + b + 1, y1);
-            st_relaxed(y + b + 2, y2);
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -407,23 +216,6 @@ void launch_fill_sentinel(uint32_t n, T* x, cudaStream_t s) {
 }
 
 template <typename T>
-void launch_trsv_nodes(const NodeSched& S, const T* lu, const T* dinv, const T* r, T* tmp, T* y,
-                       unsigned* status, int device, cudaStream_t s) {
-    if (!S.n_nodes) return;
-    static int res_lo[2] = {0, 0}, res_up[2] = {0, 0};
-    const int f = sizeof(T) == 4;
-    if (!res_lo[f]) res_lo[f] = resident_grid_nodes(k_trsv_lower_nodes<T>, device);
-    if (!res_up[f]) res_up[f] = resident_grid_nodes(k_trsv_upper_nodes<T>, device);
-    const uint32_t n = 3 * S.n_nodes;
-    k_fill_sentinel<T><<<592, 256, 0, s>>>(n, tmp);
-    k_trsv_lower_nodes<T><<<grid_for(res_lo[f], S.max_width_fwd), kNodeWarps * 32, 0, s>>>(
-        S, lu, r, tmp, status);
-    k_fill_sentinel<T><<<592, 256, 0, s>>>(n, y);
-    k_trsv_upper_nodes<T><<<grid_for(res_up[f], S.max_width_bwd), kNodeWarps * 32, 0, s>>>(
-        S, lu, dinv, tmp, y, status);
-}
-
-template <typename T>
 void launch_ilu0_nodes(const NodeSched& S, const T* a, T* lu, T* d, T* dinv, unsigned* done,
                        unsigned epoch, unsigned* status, int device, cudaStream_t s) {
     if (!S.n_nodes) return;
@@ -434,11 +226,6 @@ void launch_ilu0_nodes(const NodeSched& S, const T* a, T* lu, T* d, T* dinv, uns
         S, a, lu, d, dinv, done, epoch, status);
 }
 
-template void launch_trsv_nodes<double>(const NodeSched&, const double*, const double*,
-                                        const double*, double*, double*, unsigned*, int,
-                                        cudaStream_t);
-template void launch_trsv_nodes<float>(const NodeSched&, const float*, const float*, const float*,
-                                       float*, float*, unsigned*, int, cudaStream_t);
 template void launch_ilu0_nodes<double>(const NodeSched&, const double*, double*, double*,
                                         double*, unsigned*, unsigned, unsigned*, int,
                                         cudaStream_t);

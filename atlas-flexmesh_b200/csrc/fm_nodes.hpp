@@ -17,6 +17,9 @@ struct NodeSched {
     const uint32_t* self_pos = nullptr;  // index of n inside its own neighbour list
     const uint32_t* fwd_order = nullptr;
     const uint32_t* bwd_order = nullptr;
+    // per position of the orders: {node, nbr_ptr[node], degree, self_pos[node]}
+    const uint4* fwd_rec = nullptr;
+    const uint4* bwd_rec = nullptr;
     uint32_t max_width_fwd = 0, max_width_bwd = 0;
 };
 

@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="flexmesh", choices=["flexmesh", "reference"])
     ap.add_argument("--N", type=int, default=64)
-    ap.add_argument("--inner-tol", type=float, default=1e-3)
+    ap.add_argument("--inner-tol", type=float, default=0.1)
     ap.add_argument("--fp64-steps", type=int, default=1,
                     help="timed FP64 load steps for the mixed/FP64 comparison (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -102,7 +102,8 @@ class Clocks:
             sm = sorted(float(r[0]) for r in rows)
             mx = max(float(r[1]) for r in rows)
             names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-            reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[3 + i]})
+            reasons = sorted({names[i] for r in rows for i in range(4)
+                              if r[3 + i].strip() == "Active"})
             return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": reasons,
                     "samples": len(rows)}
         except Exception as e:  # nvidia-smi unavailable
