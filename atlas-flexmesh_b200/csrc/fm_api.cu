@@ -15,6 +15,7 @@
 
 #include "fm_api.h"
 #include "fm_kernels.hpp"
+#include "fm_adjoint.hpp"
 #include "fm_nodes.hpp"
 #include "fm_setup.hpp"
 
@@ -1227,13 +1228,116 @@ fm_status fm_profile_read(fm_ctx* c, fm_profile* out) {
     return FM_OK;
 }
 
-fm_status fm_exact_apply(fm_ctx* c, const double*, const double*, double*, int) {
-    return fail(c, FM_ERR_ARG, "fm_exact_apply: not built yet");
+fm_status fm_exact_apply(fm_ctx* c, const double* u, const double* v, double* y, int transpose) {
+    TRY(need_material(c));
+    if (!u || !v || !y) return fail(c, FM_ERR_ARG, "null argument");
+    {
+        PROF(FM_PROF_ASSEMBLE, 1);
+        fm::launch_exact_apply(mesh_view(c), u, v, y, transpose ? 1 : 0, c->stream);
+    }
+    CK(cudaGetLastError());
+    return FM_OK;
 }
 
-fm_status fm_adjoint(fm_ctx* c, const double*, const double*, double*, double*, double*, double,
-                     double, int, fm_precision, int*, int*) {
-    return fail(c, FM_ERR_ARG, "fm_adjoint: not built yet");
+// Adjoint by defect correction: the exact Jacobian K is non-symmetric, the
+// reference tangent K_t (symmetric, with its ILU(0)) is the preconditioner:
+//   w <- w + PCG(K_t, g - K^T w)   on the free DOFs, until
+//   ||g - K^T w|| <= tol ||g||.
+// FM_MIXED runs K_t, its ILU(0) and the PCG in FP32 on the scaled defect;
+// K^T w, the defect and w stay FP64, so the sweeps restore FP64 accuracy.
+fm_status fm_adjoint(fm_ctx* c, const double* u, const double* dLdu, double* gmu, double* glam,
+                     double* w_out, double tol, double inner_tol, int max_sweeps,
+                     fm_precision prec, int* sweeps_out, int* pcg_out) {
+    TRY(need_material(c));
+    if (!u || !dLdu || !gmu || !glam || max_sweeps < 1)
+        return fail(c, FM_ERR_ARG, "bad argument");
+    if (prec != FM_FP64 && prec != FM_MIXED) return fail(c, FM_ERR_ARG, "unknown precision");
+    const bool mixed = prec == FM_MIXED;
+    if (mixed) TRY(ensure_matrix<float>(c));
+    else TRY(ensure_matrix<double>(c));
+    CK(c->vec_c.reserve(c->n));
+    CK(c->vec_d.reserve(c->n));
+    CK(c->vec_e.reserve(c->n));
+    const fm::MeshDev m = mesh_view(c);
+    const uint8_t* mask = c->has_bc ? c->mask.p : nullptr;
+    double* w = w_out ? w_out : c->vec_e.p;
+    double* r = c->vec_a.p;
+    double* dw = c->vec_b.p;
+    double* y = c->vec_c.p;
+    // preconditioner: reference tangent at u, eliminated, and its ILU(0)
+    {
+        PROF(FM_PROF_ASSEMBLE, 1);
+        if (mixed) fm::launch_assemble(m, u, c->w32.K.p, nullptr, nullptr, 1, c->status(), c->stream);
+        else fm::launch_assemble(m, u, c->w64.K.p, nullptr, nullptr, 1, c->status(), c->stream);
+    }
+    if (mixed) TRY(ilu_core<float>(c, c->fem, c->w32.K.p, c->w32.LU.p, c->w32.diag.p));
+    else TRY(ilu_core<double>(c, c->fem, c->w64.K.p, c->w64.LU.p, c->w64.diag.p));
+    CK(cudaMemsetAsync(w, 0, sizeof(double) * c->n, c->stream));
+    // ||g|| on the free DOFs
+    CK(cudaMemsetAsync(y, 0, sizeof(double) * c->n, c->stream));
+    {
+        PROF(FM_PROF_VECTOR, 1);
+        fm::launch_adj_residual(c->n, mask, dLdu, y, r, c->partials.p, c->counter(),
+                                &c->sc.p->norm2, c->stream);
+    }
+    TRY(sync_scalars(c));
+    const double gn = std::sqrt(c->h_sc->norm2);
+    int sweeps = 0, pcg_total = 0;
+    bool conv = gn == 0.0;
+    double rn = gn;
+    for (; !conv && sweeps < max_sweeps; ++sweeps) {
+        int its = 0;
+        if (mixed) {
+            {
+                PROF(FM_PROF_VECTOR, 1);
+                fm::launch_to_f32_scaled(c->n, r, 1.0 / rn, c->w32.b.p, c->w32.x.p, c->stream);
+            }
+            Op<float> A{c, &c->fem, true, c->w32.K.p, c->w32.LU.p, c->w32.diag.p, c->w32.t.p,
+                        c->grid_trsv32, c->w32.dinv.p};
+            TRY(pcg_core<float>(c, A, c->n, c->w32.b.p, c->w32.x.p, inner_tol, 100000, &its,
+                                nullptr));
+            {
+                PROF(FM_PROF_VECTOR, 1);
+                fm::launch_f32_to_f64_scaled(c->n, c->w32.x.p, rn, dw, c->stream);
+            }
+        } else {
+            CK(cudaMemsetAsync(dw, 0, sizeof(double) * c->n, c->stream));
+            Op<double> A{c, &c->fem, true, c->w64.K.p, c->w64.LU.p, c->w64.diag.p, c->w64.t.p,
+                         c->grid_trsv64, c->w64.dinv.p};
+            TRY(pcg_core<double>(c, A, c->n, r, dw, inner_tol, 100000, &its, nullptr));
+        }
+        pcg_total += its;
+        {
+            PROF(FM_PROF_VECTOR, 1);
+            fm::launch_adj_update(c->n, mask, dw, w, c->stream);
+        }
+        {
+            PROF(FM_PROF_ASSEMBLE, 1);
+            fm::launch_exact_apply(m, u, w, y, 1, c->stream);
+        }
+        {
+            PROF(FM_PROF_VECTOR, 1);
+            fm::launch_adj_residual(c->n, mask, dLdu, y, r, c->partials.p, c->counter(),
+                                    &c->sc.p->norm2, c->stream);
+        }
+        TRY(sync_scalars(c));
+        TRY(check_flags(c, c->h_sc->status, "fm_adjoint"));
+        rn = std::sqrt(c->h_sc->norm2);
+        if (rn <= tol * gn) conv = true;
+    }
+    {
+        PROF(FM_PROF_ASSEMBLE, 1);
+        fm::launch_param_grads(m, u, w, gmu, glam, c->stream);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->stream));
+    c->w64.factor_valid = c->w32.factor_valid = false;
+    if (sweeps_out) *sweeps_out = sweeps;
+    if (pcg_out) *pcg_out = pcg_total;
+    if (!conv)
+        return fail(c, FM_ERR_NOT_CONVERGED, "adjoint: %d sweeps, defect %.3e of %.3e", sweeps,
+                    rn, gn);
+    return FM_OK;
 }
 
 }  // extern "C"

@@ -186,6 +186,14 @@ __device__ __forceinline__ bool tet_kinematics(const double x[12], const double 
     return true;
 }
 
+// g = dN_a for a runtime local index a, by selects (indexing the register
+// array with a runtime value would move it to local memory)
+__device__ __forceinline__ void grad_of(const TetKin& k, int a, double g[3]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        g[c] = a == 0 ? k.d[0][c] : a == 1 ? k.d[1][c] : a == 2 ? k.d[2][c] : k.d[3][c];
+}
+
 // Mandel stress M = C S with S = mu (I - C^-1) + lam ln(max(J,0.01)) C^-1
 // (neo_hookean_response, FEM/adaptive_fem_engine.hpp:79-129), evaluated in
 // the closed form M = mu (C - I) + lam lnJ I that C C^-1 = I gives; the

@@ -26,9 +26,11 @@ constexpr int kAsmWarps = 8;
 
 template <typename KT>
 struct AsmStage {
-    KT d[32][12];     // shape gradients of the 4 nodes of incident tet l
+    KT d[32][12];     // shape gradients of the 4 nodes of incident tet l; after
+                      // phase 2 reused as the [lane][9] gather of the row blocks
     KT fI[32][3];     // vol M dN_owner of tet l (force, and geometric term)
     KT vabm[32][3];   // vol*a, vol*b, vol*mu (tangent scalars)
+    double f64[3][32];  // FP64 node-force contributions of the incident tets
     uint32_t pos[32]; // 4 x u8: position of each tet node in the owner's neighbour list
     uint32_t nbr[32];
 };
@@ -100,7 +102,8 @@ __global__ void __launch_bounds__(kAsmWarps * 32)
                             lam);
                 const Mandel M = mandel_stress(k.F, k.J, mu, lam);
                 const int il = (cn[0] == n) ? 0 : (cn[1] == n) ? 1 : (cn[2] == n) ? 2 : 3;
-                const double* dI = k.d[il];
+                double dI[3];
+                grad_of(k, il, dI);
                 fi0 = k.vol * (M.m00 * dI[0] + M.m01 * dI[1] + M.m02 * dI[2]);
                 fi1 = k.vol * (M.m01 * dI[0] + M.m11 * dI[1] + M.m12 * dI[2]);
                 fi2 = k.vol * (M.m02 * dI[0] + M.m12 * dI[1] + M.m22 * dI[2]);
@@ -132,12 +135,18 @@ __global__ void __launch_bounds__(kAsmWarps * 32)
         }
     }
     S.pos[lane] = packed;
+    S.f64[0][lane] = fi0;
+    S.f64[1][lane] = fi1;
+    S.f64[2][lane] = fi2;
     if (flags) raise_flag(status, flags);
+    __syncwarp();
 
-    // internal force of the node: fixed xor-tree order, deterministic
-    const double fx = warp_sum(fi0), fy = warp_sum(fi1), fz = warp_sum(fi2);
+    // internal force of the node: lane p < 3 sums component p over the
+    // incident tets in ascending element order (deterministic).  Shared
+    // gathers replace FP64 shuffle trees, which are slow after divergence.
     if (lane < 3) {
-        const double fv = lane == 0 ? fx : (lane == 1 ? fy : fz);
+        double fv = 0.0;
+        for (int l = 0; l < mi; ++l) fv += S.f64[lane][l];
         const uint32_t row = 3 * n + lane;
         if (f) f[row] = fv;
         if (R) R[row] = (m.mask && m.mask[row]) ? 0.0 : -fv;
@@ -163,11 +172,22 @@ __global__ void __launch_bounds__(kAsmWarps * 32)
                                   S.vabm[l][1], S.vabm[l][2], acc);
         }
     }
-    // diagonal block = - sum of off-diagonal blocks of the row block
+    // diagonal block = - sum of off-diagonal blocks of the row block: lane
+    // q < 9 sums entry q over the neighbour lanes (fixed order)
+    __syncwarp();
+    KT* red = &S.d[0][0];
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        const KT s = warp_sum(acc[q]);
-        if (lane == self_k) acc[q] = -s;
+    for (int q = 0; q < 9; ++q) red[9 * lane + q] = acc[q];
+    __syncwarp();
+    if (lane < 9) {
+        KT s = KT(0);
+        for (int l = 0; l < deg; ++l) s += red[9 * l + lane];
+        red[9 * self_k + lane] = -s;
+    }
+    __syncwarp();
+    if (lane == self_k) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) acc[q] = red[9 * self_k + q];
     }
     if (lane < deg) {
         const uint32_t col0 = 3 * my_nbr;
