@@ -33,6 +33,7 @@ struct AsmStage {
     double f64[3][32];  // FP64 node-force contributions of the incident tets
     uint32_t pos[32]; // 4 x u8: position of each tet node in the owner's neighbour list
     uint32_t nbr[32];
+    uint32_t members[32];  // bit l of members[k]: tet l holds the edge (owner, nbr[k])
 };
 
 __device__ __forceinline__ int find_sorted(const uint32_t* a, int len, uint32_t key) {
@@ -57,7 +58,7 @@ __device__ __forceinline__ int byte_index(uint32_t packed, uint32_t key) {
 }
 
 template <typename KT>
-__global__ void __launch_bounds__(kAsmWarps * 32)
+__global__ void __launch_bounds__(kAsmWarps * 32, 3)
     k_assemble(MeshDev m, const double* __restrict__ u, KT* __restrict__ K,
                double* __restrict__ f, double* __restrict__ R, int apply_bc,
                unsigned* __restrict__ status) {
@@ -74,6 +75,7 @@ __global__ void __launch_bounds__(kAsmWarps * 32)
     const int mi = (int)(m.inc_ptr[n + 1] - e0);
     const uint32_t my_nbr = lane < deg ? __ldg(m.nbr + nb0 + lane) : 0xffffffffu;
     S.nbr[lane] = my_nbr;
+    S.members[lane] = 0u;
     const int self_k = __ffs(__ballot_sync(kFull, my_nbr == n)) - 1;
     __syncwarp();
 
@@ -128,6 +130,8 @@ __global__ void __launch_bounds__(kAsmWarps * 32)
                     for (int q = 0; q < 4; ++q) {
                         const int p = find_sorted(S.nbr, deg, cn[q]);
                         packed |= (uint32_t)(p < 0 ? 0xff : p) << (8 * q);
+                        // edge lists as bitmasks: fixed bit order, deterministic
+                        if (p >= 0 && p != self_k) atomicOr(&S.members[p], 1u << lane);
                     }
                     if (!isfinite(a + b)) flags |= FM_FLAG_NONFINITE;
                 }
@@ -159,9 +163,7 @@ __global__ void __launch_bounds__(kAsmWarps * 32)
 #pragma unroll
     for (int q = 0; q < 9; ++q) acc[q] = KT(0);
     if (lane < deg && lane != self_k) {
-        uint32_t members = 0;
-        for (int l = 0; l < mi; ++l)
-            if (byte_index(S.pos[l], (uint32_t)lane) >= 0) members |= 1u << l;
+        uint32_t members = S.members[lane];
         while (members) {
             const int l = __ffs(members) - 1;
             members &= members - 1;
