@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -891,6 +892,65 @@ fm_status fm_ilu0_apply(fm_ctx* c, const double* r, double* y) {
     uint32_t flags;
     TRY(device_flags(c, &flags));
     return check_flags(c, flags, "fm_ilu0_apply");
+}
+
+// ---- fm_ilu0_apply_noalloc ------------------------------------------------
+// For callers that must not allocate device memory during the call: the
+// intermediate z = L^-1 r of the two node-block solves and the status word
+// of their bounded waits live in this file-scope array instead of context
+// buffers.  One array per device for the whole process (8 MiB + 256 B, held
+// until exit); every context on the device shares it, so calls that overlap
+// on the GPU race on it.
+struct NoAllocScratch {
+    double z[FM_NOALLOC_MAX_DOFS];
+    unsigned status;
+};
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+constexpr int kNoAllocMaxDevices = 64;
+
+// Device address of g_noalloc_scratch, looked up once per device with that
+// device current.  The lookup may load the module, so the first call on a
+// device belongs before any stream capture.  (Host code must never pass
+// g_noalloc_scratch itself to a kernel: on the host that name is a stand-in,
+// not a device address.)
+static fm_status noalloc_scratch(fm_ctx* c, NoAllocScratch** out) {
+    static std::mutex mu;
+    static NoAllocScratch* addr[kNoAllocMaxDevices] = {};
+    if (c->device < 0 || c->device >= kNoAllocMaxDevices)
+        return fail(c, FM_ERR_LIMITS, "fm_ilu0_apply_noalloc: device %d beyond %d", c->device,
+                    kNoAllocMaxDevices);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[c->device]) {
+        CK(cudaSetDevice(c->device));
+        NoAllocScratch* ptr = nullptr;
+        CK(cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch));
+        addr[c->device] = ptr;
+    }
+    *out = addr[c->device];
+    return FM_OK;
+}
+
+fm_status fm_ilu0_apply_noalloc(fm_ctx* c, const double* r, double* y) {
+    TRY(need_mesh(c));
+    if (c->n > FM_NOALLOC_MAX_DOFS)
+        return fail(c, FM_ERR_LIMITS,
+                    "fm_ilu0_apply_noalloc: %u DOFs exceed the scratch limit of %u DOFs", c->n,
+                    (unsigned)FM_NOALLOC_MAX_DOFS);
+    if (!c->w64.factor_valid) return fail(c, FM_ERR_ARG, "no FP64 factorization: call fm_ilu0");
+    if (!r || !y) return fail(c, FM_ERR_ARG, "null argument");
+    NoAllocScratch* sp = nullptr;
+    TRY(noalloc_scratch(c, &sp));
+    // the status word keeps the previous call's bits: it must start at zero;
+    // z is refilled with the wait sentinel by the launcher before each solve
+    CK(cudaMemsetAsync(&sp->status, 0, sizeof(unsigned), c->stream));
+    fm::launch_trsv_nodes<double>(node_sched(c), c->w64.LU.p, c->w64.dinv.p, r, sp->z, y,
+                                  &sp->status, c->device, c->stream);
+    CK(cudaGetLastError());
+    unsigned flags = 0;
+    CK(cudaMemcpyAsync(&flags, &sp->status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return check_flags(c, flags, "fm_ilu0_apply_noalloc");
 }
 
 fm_status fm_spmv(fm_ctx* c, const double* x, double* y) {

@@ -27,7 +27,7 @@ EXPORTS = [
     "fm_unit_cube_sizes", "fm_unit_cube", "fm_set_mesh", "fm_build_pattern", "fm_set_material",
     "fm_set_material_lame", "fm_set_bc", "fm_elements", "fm_assemble", "fm_assemble_host",
     "fm_residual", "fm_assemble_reference_pattern", "fm_levels", "fm_ilu0", "fm_get_ilu0",
-    "fm_ilu0_apply", "fm_spmv", "fm_pcg", "fm_csr_pcg_ilu0", "fm_newton_solve",
+    "fm_ilu0_apply", "fm_ilu0_apply_noalloc", "fm_spmv", "fm_pcg", "fm_csr_pcg_ilu0", "fm_newton_solve",
     "fm_exact_apply", "fm_adjoint", "fm_csr_ilu0", "fm_newton_step", "fm_newton_step_host",
     "fm_profile_enable", "fm_profile_read",
 ]
@@ -79,6 +79,7 @@ def lib() -> C.CDLL:
             "fm_ilu0": [_vp, _i32],
             "fm_get_ilu0": [_vp, _vp, _vp],
             "fm_ilu0_apply": [_vp, _vp, _vp],
+            "fm_ilu0_apply_noalloc": [_vp, _vp, _vp],
             "fm_spmv": [_vp, _vp, _vp],
             "fm_pcg": [_vp, _vp, _vp, _f64, _i32, _P(_i32), _P(_f64), _i32],
             "fm_csr_pcg_ilu0": [_vp, _u32, _vp, _vp, _vp, _vp, _vp, _f64, _i32, _P(_i32),
@@ -284,6 +285,14 @@ class Context:
     def ilu0_apply(self, r):
         y = self._zeros(self.n_dofs)
         self._check(lib().fm_ilu0_apply(self._h, _dp(r), _dp(y)), "fm_ilu0_apply")
+        return y
+
+    def ilu0_apply_noalloc(self, r, y):
+        """fm_ilu0_apply into the caller's y without any allocation in the call
+        (library-owned static scratch, at most 2**20 DOFs, one call at a time
+        per device)."""
+        self._check(lib().fm_ilu0_apply_noalloc(self._h, _dp(r), _dp(y)),
+                    "fm_ilu0_apply_noalloc")
         return y
 
     def spmv(self, x):

@@ -47,7 +47,7 @@ typedef enum {
     FM_ERR_INVERTED = 6,       /* reserved: det F <= 0 is reported as a flag */
     FM_ERR_TIMEOUT = 7,        /* a bounded device wait expired */
     FM_ERR_NOT_CONVERGED = 8,  /* Newton/PCG stopped at its iteration cap */
-    FM_ERR_LIMITS = 9          /* mesh valence beyond the kernels' limits */
+    FM_ERR_LIMITS = 9          /* mesh valence or size beyond the kernels' limits */
 } fm_status;
 
 typedef enum { FM_FP64 = 0, FM_MIXED = 1 } fm_precision;
@@ -191,6 +191,21 @@ fm_status fm_ilu0(fm_ctx* ctx, fm_precision prec);
 fm_status fm_get_ilu0(fm_ctx* ctx, double* LU_host, double* diag_host);
 /* Replaces ILU0Preconditioner::solve (:473-504): y = U^-1 L^-1 r. */
 fm_status fm_ilu0_apply(fm_ctx* ctx, const double* r_dev, double* y_dev);
+/* No counterpart in the reference.  fm_ilu0_apply for callers that must not
+ * allocate device memory during the call (an application whose HBM belongs
+ * to another allocator, where a cudaMalloc can fail, or that cannot take
+ * the device-wide synchronization of cudaFree): the intermediate L^-1 r and
+ * the wait-status word live in one file-scope device array of the library
+ * (FM_NOALLOC_MAX_DOFS doubles = 8 MiB, held by every GPU that loads the
+ * library until exit), not in context buffers.  Meshes with more than
+ * FM_NOALLOC_MAX_DOFS DOFs are rejected with FM_ERR_LIMITS.  The first call
+ * on a device looks the array up (cudaGetSymbolAddress): make that first
+ * call before any stream capture.  Every context on a device shares the
+ * array: calls that overlap on the GPU race, so issue one at a time per
+ * device.  Output is bit-identical to fm_ilu0_apply's.  Synchronizes the
+ * context's stream. */
+#define FM_NOALLOC_MAX_DOFS (1u << 20)
+fm_status fm_ilu0_apply_noalloc(fm_ctx* ctx, const double* r_dev, double* y_dev);
 
 /* ---- A17/A18: SpMV and PCG on the context's K -----------------------------
  * fm_spmv replaces SparseCSR::matvec (FEM/fem_types.hpp:310-319).
