@@ -1,0 +1,341 @@
+"""Single-kernel cases and the per-workload runs, for profiling and reports.
+
+    python -m flexmesh_b200.cases trsv     --N 64 --prec mixed --applies 4
+    python -m flexmesh_b200.cases ilu      --N 64 --prec fp64 --reps 2
+    python -m flexmesh_b200.cases assemble --N 128 --prec fp64 --reps 5
+    python -m flexmesh_b200.cases adjoint  --N 32 --fd 64
+    python -m flexmesh_b200.cases incompressible --N 48
+
+(with ``atlas-flexmesh_b200`` on ``PYTHONPATH``).  Every case prints one JSON
+line.  ``trsv``, ``ilu`` and ``assemble`` are sized for ``ncu`` captures: one
+context, a few launches of the kernel of interest after a short set-up, and
+device timings from CUDA events on the context's stream.  ``adjoint`` and
+``incompressible`` are the material-gradient check on the 32^3 block and the
+near-incompressible 48^3 run (nu = 0.49, 20 load steps).
+
+Algorithmic bytes per launch (what the roofline fractions count; schedule
+records, neighbour lists and recomputation are not counted):
+  assembly   24 E + 48 Nn + w nnz + 8 n       (conn + E_e, X and u, K, f_int)
+  ILU(0)     (2w + 4) nnz + 4 (n + 1)
+  solves     (w + 4)(nnz - n) + w n + 8 (n + 1) + 4 w n   (forward + backward)
+with E tets, Nn nodes, n = 3 Nn DOFs, w = 8 (FP64) or 4 (FP32).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from . import configs
+
+PREC = {"fp64": L.FM_FP64, "mixed": L.FM_MIXED}
+
+
+def hbm_peak():
+    """measured copy bandwidth of this GPU pool (GB/s) when the repository
+    carries MEASURED_PEAKS.json, else the fallback figure"""
+    here = os.path.dirname(os.path.abspath(__file__))
+    path = os.path.join(here, "..", "..", "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def bytes_assembly(E, Nn, nnz, w):
+    return 24 * E + 48 * Nn + w * nnz + 8 * 3 * Nn
+
+
+def bytes_ilu(nnz, n, w):
+    return (2 * w + 4) * nnz + 4 * (n + 1)
+
+
+def bytes_solves(nnz, n, w):
+    return (w + 4) * (nnz - n) + w * n + 8 * (n + 1) + 4 * w * n
+
+
+def problem_context(P, device=0):
+    ctx = L.Context(device)
+    ctx.set_mesh(P.xyz, P.conn, P.elem_volume)
+    ctx.set_material(P.E, P.nu, P.E_elem)
+    ctx.set_bc(P.mask, P.bc_value)
+    return ctx
+
+
+class Timer:
+    """CUDA-event interval on the given stream"""
+
+    def __init__(self, stream):
+        self.s = stream
+        self.a = torch.cuda.Event(enable_timing=True)
+        self.b = torch.cuda.Event(enable_timing=True)
+
+    def __enter__(self):
+        torch.cuda.synchronize()
+        self.a.record(self.s)
+        return self
+
+    def __exit__(self, *exc):
+        self.b.record(self.s)
+        torch.cuda.synchronize()
+        self.ms = self.a.elapsed_time(self.b)
+
+
+def case_trsv(a):
+    """Forward + backward solves of ILU(0) on the scale-up block's tangent
+    at u = 0 (Dirichlet rows eliminated).  FP64 applies go through
+    fm_ilu0_apply; FP32 ones through fm_pcg in mixed precision, whose
+    iterations each make one apply (plus one SpMV and vector updates)."""
+    P = configs.scaleup_block(a.N)
+    ctx = problem_context(P)
+    n = ctx.n_dofs
+    u = torch.zeros(n, dtype=torch.float64, device="cuda")
+    prec = PREC[a.prec]
+    ctx.assemble_into_context(u, prec=prec, apply_bc=True)
+    ctx.ilu0(prec)
+    r = torch.as_tensor(np.random.default_rng(5).standard_normal(n), device="cuda")
+    r[torch.as_tensor(P.mask, device="cuda") == 1] = 0.0
+    ctx.profile_enable(True)
+    with Timer(ctx.stream) as t:
+        if prec == L.FM_FP64:
+            for _ in range(a.applies):
+                ctx.ilu0_apply(r)
+        else:
+            ctx.pcg(r, tol=1e-30, max_iter=max(a.applies - 1, 0), prec=prec)
+    prof = ctx.profile_read()
+    w = 8 if prec == L.FM_FP64 else 4
+    p = prof["trsv"]
+    per = p["ms"] / max(p["calls"], 1)
+    B = bytes_solves(ctx.nnz, n, w)
+    peak, kind = hbm_peak()
+    return {"case": "trsv", "N": a.N, "prec": a.prec, "applies": p["calls"],
+            "ms_per_apply": round(per, 4), "bytes_per_apply": B,
+            "achieved_gbs": round(B / per / 1e6, 1), "peak_gbs": peak, "peak_kind": kind,
+            "frac": round(B / per / 1e6 / peak, 4), "wall_ms": round(t.ms, 2)}
+
+
+def case_ilu(a):
+    """ILU(0) factorizations of the scale-up block's tangent at u = 0"""
+    P = configs.scaleup_block(a.N)
+    ctx = problem_context(P)
+    n = ctx.n_dofs
+    u = torch.zeros(n, dtype=torch.float64, device="cuda")
+    prec = PREC[a.prec]
+    ctx.assemble_into_context(u, prec=prec, apply_bc=True)
+    ctx.profile_enable(True)
+    for _ in range(a.reps):
+        ctx.ilu0(prec)
+    prof = ctx.profile_read()["ilu0"]
+    w = 8 if prec == L.FM_FP64 else 4
+    per = prof["ms"] / max(prof["calls"], 1)
+    B = bytes_ilu(ctx.nnz, n, w)
+    peak, kind = hbm_peak()
+    return {"case": "ilu", "N": a.N, "prec": a.prec, "reps": prof["calls"],
+            "ms_per_factorization": round(per, 3), "bytes": B,
+            "achieved_gbs": round(B / per / 1e6, 1), "peak_gbs": peak, "peak_kind": kind,
+            "frac": round(B / per / 1e6 / peak, 4)}
+
+
+def case_assemble(a):
+    """One residual + tangent + CSR scatter of the assembly block (128^3 x 6
+    tets: sinusoidal displacement, log-normal mu), timed per call.  The K of
+    consecutive calls (2.9 GB FP64, 1.4 GB FP32 at N=128) exceeds the L2, so
+    each call streams from HBM."""
+    P = configs.assembly_block(a.N)
+    ctx = problem_context(P)
+    prec = PREC[a.prec]
+    u = torch.as_tensor(P.meta["u"], device="cuda")
+    f = torch.zeros_like(u)
+    for _ in range(a.warmup):
+        ctx.assemble_into_context(u, prec=prec, apply_bc=False, f=f)
+    times = []
+    for _ in range(a.reps):
+        with Timer(ctx.stream) as t:
+            ctx.assemble_into_context(u, prec=prec, apply_bc=False, f=f)
+        times.append(t.ms)
+    ms = float(np.median(times))
+    w = 8 if prec == L.FM_FP64 else 4
+    B = bytes_assembly(ctx.n_elems, ctx.n_nodes, ctx.nnz, w)
+    peak, kind = hbm_peak()
+    return {"case": "assemble", "N": a.N, "prec": a.prec, "tets": ctx.n_elems,
+            "ms_median": round(ms, 3), "ms_min": round(min(times), 3),
+            "tets_per_s": round(ctx.n_elems / ms * 1e3, 1), "bytes": B,
+            "achieved_gbs": round(B / ms / 1e6, 1), "peak_gbs": peak, "peak_kind": kind,
+            "frac": round(B / ms / 1e6 / peak, 4),
+            "flags": ctx.flags()}
+
+
+def _solve_path(ctx, n, n_steps, prec, inner_tol, rtol=1e-10, u0=None, steps=None,
+                line_search=0, max_newton=400):
+    u = torch.zeros(n, dtype=torch.float64, device="cuda") if u0 is None else u0.clone()
+    newton, pcg, per_step = 0, 0, []
+    for s in (steps if steps is not None else range(1, n_steps + 1)):
+        r = ctx.newton_step(u, s / n_steps, rtol=rtol, inner_tol=inner_tol,
+                            max_newton=max_newton, max_pcg=20000, line_search=line_search,
+                            prec=prec, allow_not_converged=max_newton < 400)
+        newton += r["newton_iters"]
+        pcg += r["pcg_iters"]
+        per_step.append((r["newton_iters"], r["pcg_iters"]))
+    return u, newton, pcg, per_step
+
+
+def case_adjoint(a):
+    """Material gradients of L = 1/2 |u_top(mu) - u*|^2 on the 32^3 block:
+    u* from the 'true' log-normal mu (seed A), the model mu from seed B.
+    FP64 and mixed adjoints against central finite differences
+    (step 1e-6 mu_e, lambda_e) on a.fd seeded elements.  The finite
+    differences re-solve from the converged state at full load (the
+    material is hyperelastic, so the equilibrium does not depend on the
+    path) with three Newton iterations (the perturbation is linear to
+    O(h^2), and the first iteration already solves it to the PCG
+    tolerance), and the loss difference is formed as
+    1/2 sum (a+ - a-)(a+ + a- - 2 u*), which keeps the cancellation of the
+    two nearby losses out of the quotient."""
+    P = configs.adjoint_block(a.N)
+    nu = P.nu
+    ctx = problem_context(P)
+    n = ctx.n_dofs
+    sel = torch.as_tensor(configs.top_face_xy_dofs(P.xyz), device="cuda")
+    mu_m, lam_m = P.lame()
+    Et = P.meta["E_true"]
+    mu_t = Et / (2 * (1 + nu))
+    lam_t = Et * nu / ((1 + nu) * (1 - 2 * nu))
+    # target from the true field
+    ctx.set_material_lame(mu_t, lam_t, nu)
+    u_t, *_ = _solve_path(ctx, n, P.n_steps, L.FM_FP64, 1e-12, rtol=1e-12)
+    target = u_t[sel].clone()
+    ctx.set_material_lame(mu_m, lam_m, nu)
+    t0 = time.perf_counter()
+    u, nw, npcg, _ = _solve_path(ctx, n, P.n_steps, L.FM_FP64, 1e-12, rtol=1e-12)
+    t_fwd = time.perf_counter() - t0
+
+    def loss(uu):
+        return 0.5 * float(torch.sum((uu[sel] - target) ** 2))
+
+    g = torch.zeros_like(u)
+    g[sel] = u[sel] - target
+    res = {"case": "adjoint", "N": a.N, "tets": ctx.n_elems, "forward_s": round(t_fwd, 3),
+           "forward_newton": nw, "forward_pcg": npcg, "loss": loss(u)}
+    grads = {}
+    for name, prec, inner in (("fp64", L.FM_FP64, 1e-12), ("mixed", L.FM_MIXED, 0.1)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gm, gl, _, sweeps, pit = ctx.adjoint(u, g, tol=1e-11, inner_tol=inner, prec=prec)
+        torch.cuda.synchronize()
+        grads[name] = (gm.cpu().numpy(), gl.cpu().numpy())
+        res[f"adjoint_{name}"] = {"s": round(time.perf_counter() - t0, 3), "sweeps": sweeps,
+                                  "pcg": pit}
+    g64, g32 = grads["fp64"], grads["mixed"]
+    res["mixed_vs_fp64_rel"] = {
+        "mu": float(np.linalg.norm(g32[0] - g64[0]) / np.linalg.norm(g64[0])),
+        "lam": float(np.linalg.norm(g32[1] - g64[1]) / np.linalg.norm(g64[1]))}
+    # central finite differences on seeded active elements
+    active = np.nonzero(P.elem_volume >= 1e-30)[0]
+    pick = np.sort(np.random.default_rng(configs.SEED_FD_4).choice(active, a.fd, replace=False))
+    errs = {"fp64": [], "mixed": []}
+    rows = []
+    t0 = time.perf_counter()
+    for e in pick:
+        for pname in ("mu", "lam"):
+            base = mu_m if pname == "mu" else lam_m
+            h = 1e-6 * base[e]
+            tops = []
+            for sgn in (1.0, -1.0):
+                p = base.copy()
+                p[e] += sgn * h
+                ctx.set_material_lame(p if pname == "mu" else mu_m,
+                                      p if pname == "lam" else lam_m, nu)
+                up, *_ = _solve_path(ctx, n, 1, L.FM_FP64, 1e-13, rtol=1e-30, u0=u,
+                                     steps=[1], max_newton=3)
+                tops.append(up[sel])
+            dl = 0.5 * float(torch.sum((tops[0] - tops[1]) * (tops[0] + tops[1] - 2 * target)))
+            fd = dl / (2 * h)
+            k = 0 if pname == "mu" else 1
+            for name in ("fp64", "mixed"):
+                ge = float(grads[name][k][e])
+                errs[name].append(abs(ge - fd) / max(abs(fd), 1e-300))
+            rows.append((int(e), pname, fd, float(grads["fp64"][k][e])))
+    ctx.set_material_lame(mu_m, lam_m, nu)
+    res["fd_s"] = round(time.perf_counter() - t0, 1)
+    res["fd_elements"] = int(a.fd)
+    res["fd_rel_err"] = {name: {"max": float(np.max(v)), "median": float(np.median(v)),
+                                "n_above_1e-6": int(np.sum(np.asarray(v) > 1e-6))}
+                         for name, v in errs.items()}
+    res["fd_sample"] = [{"e": r[0], "p": r[1], "fd": r[2], "adj": r[3]} for r in rows[:4]]
+    return res
+
+
+def case_incompressible(a):
+    """Near-incompressible block (48^3 x 6 tets, jitter 0.1 h, nu = 0.49,
+    u_z = -0.4 in 20 load steps): mixed-precision Newton against FP64, PCG
+    iterations per load step, and the adjoint dL/dmu for
+    L = 1/2 |u_top - u*|^2 with u* from a log-normal mu field (sigma 0.2)."""
+    P = configs.near_incompressible_block(a.N)
+    nu = P.nu
+    ctx = problem_context(P)
+    n = ctx.n_dofs
+    out = {"case": "incompressible", "N": a.N, "tets": ctx.n_elems, "nu": nu,
+           "load_steps": P.n_steps}
+    runs = {}
+    for name, prec, inner in (("fp64", L.FM_FP64, 1e-12), ("mixed", L.FM_MIXED, a.inner_tol)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        u, nw, npcg, per = _solve_path(ctx, n, P.n_steps, prec, inner,
+                                       line_search=a.line_search)
+        torch.cuda.synchronize()
+        runs[name] = u
+        out[name] = {"s": round(time.perf_counter() - t0, 2), "newton": nw, "pcg": npcg,
+                     "pcg_per_newton_by_step": [round(p / max(k, 1), 1) for k, p in per],
+                     "newton_by_step": [k for k, _ in per]}
+    out["mixed_vs_fp64_rel"] = float(torch.linalg.norm(runs["mixed"] - runs["fp64"]) /
+                                     torch.linalg.norm(runs["fp64"]))
+    # adjoint of the top-face loss against u* from the log-normal field
+    sel = torch.as_tensor(configs.top_face_xy_dofs(P.xyz), device="cuda")
+    Et = P.meta["E_true"]
+    ctx.set_material(P.E, nu, Et)
+    u_t, *_ = _solve_path(ctx, n, P.n_steps, L.FM_MIXED, a.inner_tol,
+                          line_search=a.line_search)
+    ctx.set_material(P.E, nu, P.E_elem)
+    u = runs["fp64"]
+    g = torch.zeros_like(u)
+    g[sel] = u[sel] - u_t[sel]
+    gm64, _, _, s64, p64 = ctx.adjoint(u, g, tol=1e-11, inner_tol=1e-12, prec=L.FM_FP64)
+    gm32, _, _, s32, p32 = ctx.adjoint(u, g, tol=1e-11, inner_tol=0.1, prec=L.FM_MIXED)
+    out["adjoint"] = {"fp64_sweeps": s64, "fp64_pcg": p64, "mixed_sweeps": s32,
+                      "mixed_pcg": p32,
+                      "dLdmu_norm": float(torch.linalg.norm(gm64)),
+                      "mixed_vs_fp64_rel": float(torch.linalg.norm(gm32 - gm64) /
+                                                 torch.linalg.norm(gm64))}
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(prog="python -m flexmesh_b200.cases")
+    ap.add_argument("case", choices=["trsv", "ilu", "assemble", "adjoint", "incompressible"])
+    ap.add_argument("--N", type=int, default=None)
+    ap.add_argument("--prec", choices=list(PREC), default="fp64")
+    ap.add_argument("--applies", type=int, default=4)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=2)
+    ap.add_argument("--fd", type=int, default=64)
+    ap.add_argument("--inner-tol", type=float, default=0.1)
+    ap.add_argument("--line-search", type=int, default=0)
+    a = ap.parse_args(argv)
+    if not torch.cuda.is_available():
+        raise SystemExit("cases need a CUDA device")
+    default_N = {"trsv": 64, "ilu": 64, "assemble": 128, "adjoint": 32, "incompressible": 48}
+    if a.N is None:
+        a.N = default_N[a.case]
+    fn = {"trsv": case_trsv, "ilu": case_ilu, "assemble": case_assemble,
+          "adjoint": case_adjoint, "incompressible": case_incompressible}[a.case]
+    print(json.dumps(fn(a)), flush=True)
+
+
+if __name__ == "__main__":
+    main()
