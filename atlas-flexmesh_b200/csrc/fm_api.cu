@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -98,9 +99,18 @@ struct fm_ctx {
     SolverCsr fem;   // solve pattern of the mesh
     SolverCsr gen;   // generic CSR (fm_csr_pcg_ilu0)
     // node-block schedule of the solve pattern (ILU(0) and triangular solves)
-    DevBuf<uint32_t> self_pos, node_fwd, node_bwd;
+    DevBuf<uint32_t> self_pos, node_fwd, node_bwd, emap_ptr;
+    DevBuf<uint8_t> emap;  // ILU(0) update map
     DevBuf<uint4> node_fwd_rec, node_bwd_rec;
     uint32_t node_levels_fwd = 0, node_levels_bwd = 0, width_fwd = 0, width_bwd = 0;
+    // cluster-synchronous solves (fm_trsv_cluster.cu): plans of both
+    // directions and whether the device runs them in FP32 / FP64
+    DevBuf<uint32_t> cl_lvl_f, cl_lvl_b, cl_nslot, cl_rptr_f, cl_rptr_b, cl_reset_f, cl_reset_b;
+    DevBuf<uint4> cl_rec_f, cl_rec_b;
+    DevBuf<uint32_t> cl_card_f, cl_card_b;  // card index of every position
+    DevBuf<unsigned char> cl_pack32_f, cl_pack32_b, cl_pack64_f, cl_pack64_b;
+    fm::ClusterSolve cl_f, cl_b;
+    bool cl_ok32 = false, cl_ok64 = false;
     std::vector<uint32_t> lvl_fwd_ptr, lvl_fwd_rows, lvl_bwd_ptr, lvl_bwd_rows;
 
     // material
@@ -364,7 +374,109 @@ fm::NodeSched node_sched(const fm_ctx* c) {
     S.bwd_rec = c->node_bwd_rec.p;
     S.max_width_fwd = c->width_fwd;
     S.max_width_bwd = c->width_bwd;
+    S.emap_ptr = c->emap_ptr.p;
+    S.emap = c->emap.p;
     return S;
+}
+
+// Plans for the cluster solves: the largest cluster (16, then 8 CTAs of 32
+// warps) whose plan fits and that the device can make resident.  Selected
+// with FM_TRSV_PATH=cluster in the environment; the grid-wide pipelined
+// solves are the default.
+fm_status setup_cluster_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
+                               const std::vector<uint32_t>& lo, const std::vector<uint32_t>& up,
+                               const std::vector<uint32_t>& uo) {
+    c->cl_ok32 = c->cl_ok64 = false;
+    const char* path = getenv("FM_TRSV_PATH");
+    if (!path || std::strcmp(path, "cluster") != 0) return FM_OK;
+    constexpr uint32_t kWarps = 32, kMaxSlots = 4096;
+    constexpr size_t kMaxSmem = 227 * 1024;
+    const char* wenv = getenv("FM_TRSV_WINDOW");
+    const uint32_t window = wenv ? std::max(1u, (uint32_t)strtoul(wenv, nullptr, 10)) : 8u;
+    for (uint32_t cs : {16u, 8u}) {
+        fm::ClusterPlan pf, pb;
+        std::vector<uint32_t> nslot;
+        if (!fm::cluster_plan(c->graph, true, lp, lo, cs, kWarps, window, kMaxSlots, pf, nslot) ||
+            !fm::cluster_plan(c->graph, false, up, uo, cs, kWarps, window, kMaxSlots, pb, nslot))
+            continue;
+        if (pf.max_per_warp > 32 || pb.max_per_warp > 32) continue;
+        auto view = [](const fm::ClusterPlan& p) {
+            fm::ClusterSolve v;
+            v.n_levels = p.n_levels;
+            v.n_ctas = p.n_ctas;
+            v.warps_per_cta = p.warps_per_cta;
+            v.max_per_warp = std::max(p.max_per_warp, 1u);
+            v.maxc = std::max(p.max_cnt, 1u);
+            v.pool_slots = std::max(p.slots_per_cta, 1u);
+            v.window = p.window;
+            return v;
+        };
+        fm::ClusterSolve f = view(pf), b = view(pb);
+        auto fits = [&](size_t vb) {
+            const int st = fm::cluster_stages(vb);
+            const size_t sm = std::max(fm::cluster_smem_bytes(f, vb, st),
+                                       fm::cluster_smem_bytes(b, vb, st));
+            return sm <= kMaxSmem && fm::cluster_max_active(vb, (int)cs, sm) >= 1;
+        };
+        const bool ok32 = fits(4), ok64 = fits(8);
+        if (!ok32 && !ok64) continue;
+        CK(upload(c->cl_lvl_f, pf.lvl_ptr.data(), pf.lvl_ptr.size(), c->stream));
+        CK(upload(c->cl_lvl_b, pb.lvl_ptr.data(), pb.lvl_ptr.size(), c->stream));
+        CK(upload(c->cl_rec_f, reinterpret_cast<const uint4*>(pf.rec.data()), pf.rec.size() / 4,
+                  c->stream));
+        CK(upload(c->cl_rec_b, reinterpret_cast<const uint4*>(pb.rec.data()), pb.rec.size() / 4,
+                  c->stream));
+        CK(upload(c->cl_nslot, nslot.data(), nslot.size(), c->stream));
+        CK(upload(c->cl_rptr_f, pf.reset_ptr.data(), pf.reset_ptr.size(), c->stream));
+        CK(upload(c->cl_rptr_b, pb.reset_ptr.data(), pb.reset_ptr.size(), c->stream));
+        CK(upload(c->cl_reset_f, pf.reset.data(), pf.reset.size(), c->stream));
+        CK(upload(c->cl_reset_b, pb.reset.data(), pb.reset.size(), c->stream));
+        std::vector<uint32_t> card;
+        fm::cluster_card_index(pf.lvl_ptr, cs * kWarps, card);
+        CK(upload(c->cl_card_f, card.data(), card.size(), c->stream));
+        fm::cluster_card_index(pb.lvl_ptr, cs * kWarps, card);
+        CK(upload(c->cl_card_b, card.data(), card.size(), c->stream));
+        f.lvl_ptr = c->cl_lvl_f.p;
+        f.rec = c->cl_rec_f.p;
+        f.nslot = c->cl_nslot.p;
+        f.reset_ptr = c->cl_rptr_f.p;
+        f.reset = c->cl_reset_f.p;
+        b.lvl_ptr = c->cl_lvl_b.p;
+        b.rec = c->cl_rec_b.p;
+        b.nslot = c->cl_nslot.p;
+        b.reset_ptr = c->cl_rptr_b.p;
+        b.reset = c->cl_reset_b.p;
+        c->cl_f = f;
+        c->cl_b = b;
+        c->cl_ok32 = ok32;
+        c->cl_ok64 = ok64;
+        CK(cudaStreamSynchronize(c->stream));
+        return FM_OK;
+    }
+    return FM_OK;
+}
+
+// z = U^-1 L^-1 r on the node-block factors (tmp: the intermediate); the
+// cluster-synchronous solves where the context has them, else the
+// grid-wide pipelined ones.  Returns the kernels launched.
+template <typename T>
+DevBuf<unsigned char>& packed_cards(fm_ctx* c, bool fwd);
+
+template <typename T>
+int precond_nodes(fm_ctx* c, const T* lu, const T* dinv, const T* r, T* tmp, T* z,
+                  unsigned* status) {
+    const bool cl = sizeof(T) == 4 ? c->cl_ok32 : c->cl_ok64;
+    if (cl && c->nn) {
+        if (fm::launch_trsv_cluster<T>(c->cl_f, c->cl_b, packed_cards<T>(c, true).p,
+                                       packed_cards<T>(c, false).p, r, tmp, z, status,
+                                       c->stream) == cudaSuccess)
+            return 2;
+        // a launch the device refuses: the pipelined solves from now on
+        cudaGetLastError();
+        c->cl_ok32 = c->cl_ok64 = false;
+    }
+    fm::launch_trsv_nodes<T>(node_sched(c), lu, dinv, r, tmp, z, status, c->device, c->stream);
+    return 4;
 }
 
 // A linear operator for PCG: the mesh K (node-block SpMV) or a generic CSR.
@@ -390,10 +502,10 @@ struct Op {
                                    c->stream);
     }
     void precond(const T* r, T* z) const {
-        PROF(FM_PROF_TRSV, node_block ? 4 : 2);
+        const bool cl = node_block && (sizeof(T) == 4 ? c->cl_ok32 : c->cl_ok64);
+        PROF(FM_PROF_TRSV, node_block && !cl ? 4 : 2);
         if (node_block) {
-            fm::launch_trsv_nodes<T>(node_sched(c), LU, dinv, r, tmp, z, c->status(), c->device,
-                                     c->stream);
+            precond_nodes<T>(c, LU, dinv, r, tmp, z, c->status());
             return;
         }
         const fm::CsrDev v = S->view();
@@ -447,12 +559,29 @@ fm_status pcg_core(fm_ctx* c, const Op<T>& A, uint32_t n, const T* b, T* x, doub
 }
 
 template <typename T>
+DevBuf<unsigned char>& packed_cards(fm_ctx* c, bool fwd) {
+    if (sizeof(T) == 4) return fwd ? c->cl_pack32_f : c->cl_pack32_b;
+    return fwd ? c->cl_pack64_f : c->cl_pack64_b;
+}
+
+template <typename T>
 fm_status ilu_core(fm_ctx* c, SolverCsr& S, const T* a, T* lu, T* diag) {
-    PROF(FM_PROF_ILU, 1);
+    const bool cl = &S == &c->fem && (sizeof(T) == 4 ? c->cl_ok32 : c->cl_ok64);
+    PROF(FM_PROF_ILU, cl ? 3 : 1);
     if (&S == &c->fem) {
         fm::launch_ilu0_nodes<T>(node_sched(c), a, lu, diag, work<T>(c).dinv.p, c->done.p,
                                  next_epoch(c), c->status(), c->device, c->stream);
         CK(cudaGetLastError());
+        if (cl) {
+            // the cluster solves read the factors as packed cards
+            DevBuf<unsigned char>& pf = packed_cards<T>(c, true);
+            DevBuf<unsigned char>& pb = packed_cards<T>(c, false);
+            CK(pf.reserve((size_t)c->nn * fm::cluster_card_bytes(c->cl_f, sizeof(T))));
+            CK(pb.reserve((size_t)c->nn * fm::cluster_card_bytes(c->cl_b, sizeof(T))));
+            fm::launch_pack_cards<T>(c->cl_f, c->cl_b, c->cl_card_f.p, c->cl_card_b.p, c->nn, lu,
+                                     work<T>(c).dinv.p, pf.p, pb.p, c->stream);
+            CK(cudaGetLastError());
+        }
         return FM_OK;
     }
     const fm::CsrDev v = S.view();
@@ -639,6 +768,13 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
             for (size_t l = 0; l + 1 < up.size(); ++l)
                 c->width_bwd = std::max(c->width_bwd, up[l + 1] - up[l]);
             CK(upload(c->self_pos, c->graph.self.data(), c->graph.self.size(), c->stream));
+            {
+                std::vector<uint32_t> ep;
+                std::vector<uint8_t> em;
+                fm::ilu_edge_maps(c->graph, ep, em);
+                CK(upload(c->emap_ptr, ep.data(), ep.size(), c->stream));
+                CK(upload(c->emap, em.data(), em.size(), c->stream));
+            }
             CK(upload(c->node_fwd, lo.data(), lo.size(), c->stream));
             CK(upload(c->node_bwd, uo.data(), uo.size(), c->stream));
             // one 16-byte schedule record per position of each order
@@ -654,6 +790,7 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
             const std::vector<uint4> rf = records(lo), rb = records(uo);
             CK(upload(c->node_fwd_rec, rf.data(), rf.size(), c->stream));
             CK(upload(c->node_bwd_rec, rb.data(), rb.size(), c->stream));
+            TRY(setup_cluster_solves(c, lp, lo, up, uo));
             CK(cudaStreamSynchronize(c->stream));
             CK(c->done.reserve(std::max<size_t>(c->done.n, (size_t)c->nn + 1)));
             CK(cudaMemsetAsync(c->done.p, 0, c->done.n * sizeof(unsigned), c->stream));
@@ -944,8 +1081,7 @@ fm_status fm_ilu0_apply_noalloc(fm_ctx* c, const double* r, double* y) {
     // the status word keeps the previous call's bits: it must start at zero;
     // z is refilled with the wait sentinel by the launcher before each solve
     CK(cudaMemsetAsync(&sp->status, 0, sizeof(unsigned), c->stream));
-    fm::launch_trsv_nodes<double>(node_sched(c), c->w64.LU.p, c->w64.dinv.p, r, sp->z, y,
-                                  &sp->status, c->device, c->stream);
+    precond_nodes<double>(c, c->w64.LU.p, c->w64.dinv.p, r, sp->z, y, &sp->status);
     CK(cudaGetLastError());
     unsigned flags = 0;
     CK(cudaMemcpyAsync(&flags, &sp->status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));

@@ -19,7 +19,7 @@
 
 namespace fm {
 
-constexpr int kNodeWarps = 8;
+constexpr int kNodeWarps = 4;
 
 template <typename T>
 __global__ void k_fill_sentinel(uint32_t n, T* __restrict__ x) {
@@ -35,63 +35,38 @@ __global__ void k_fill_sentinel(uint32_t n, T* __restrict__ x) {
 // pattern; the pivot of row 3n+p is w_p[3n+p] after all its updates,
 // perturbed by +-1e-8 when below 1e-12 in magnitude.  The subtraction order
 // per entry is the reference's (ascending c).
-// Shared memory per warp: the node's 3 rows (3*3*deg values), its
-// neighbour list, and the position map of neighbour m's upper neighbours.
+//
+// The node's three rows live in registers (lane owns columns lane,
+// lane+32, lane+64).  Once every lower neighbour's rows are final, their U
+// parts are staged into shared memory in one round of independent loads,
+// already scattered to the node's own column positions through a
+// structural map built on the host (ilu_edge_maps): a dense row per
+// (neighbour, row q), zero where the neighbour has no entry.  Each
+// elimination step is then a broadcast of the pivot column (three
+// shuffles) and three FMAs per owned column, with no shared-memory
+// read-modify-write and no warp barrier.  Neighbours are staged in chunks
+// that fit kUStage bytes.
 // ---------------------------------------------------------------------------
+constexpr int kUStage = 11264;  // bytes of dense U rows staged per warp
+constexpr int kPairRound = 3;   // (neighbour, node) pairs each lane loads per round
+
 template <typename T>
 struct IluStage {
-    T w[3][3 * 32];       // rows p of node n, entries [k][q] flattened, deg <= 32
-    uint32_t nbr[32];     // neighbours of n
-};
-
-// U part of the three rows of lower neighbour m, held in registers: lane
-// owns column j = 3*msk + 1 + lane (+32) of m's rows, with its destination
-// in n's rows (-1 when n's pattern lacks that column).
-template <typename T>
-struct URows {
-    T u[2][3];
-    int dst[2];
-    int jj[2];
-    T dinv[3];
+    T u[kUStage / sizeof(T)];  // [k - k0][q][column of n] U(3m+q, .) of staged neighbours
+    uint32_t poff[33];         // first pair of lower neighbour k (m, then its upper neighbours)
+    uint32_t mb0[32];          // lower neighbour k: first neighbour entry
+    uint8_t mdeg[32], msk[32];
 };
 
 template <typename T>
-__device__ __forceinline__ void load_urows(const NodeSched& S, const T* lu, const T* dinv,
-                                           const uint32_t* nbr_n, int deg, uint32_t m, int lane,
-                                           URows<T>& U) {
-    const uint32_t mb0 = __ldg(S.nbr_ptr + m);
-    const int mdeg = (int)(__ldg(S.nbr_ptr + m + 1) - mb0);
-    const int msk = (int)__ldg(S.self_pos + m);
-    const int mrl = 3 * mdeg;
-    const T* urow = lu + 9 * (size_t)mb0;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int j = 3 * msk + 1 + lane + 32 * h;
-        U.jj[h] = j;
-        U.dst[h] = -1;
-        U.u[h][0] = U.u[h][1] = U.u[h][2] = T(0);
-        if (j < mrl) {
-            const int kk = j / 3;
-            const uint32_t mm = __ldg(S.nbr + mb0 + kk);
-            int lo = 0, hi = deg - 1, pos = -1;
-            while (lo <= hi) {
-                const int mid = (lo + hi) >> 1;
-                const uint32_t v = nbr_n[mid];
-                if (v == mm) { pos = mid; break; }
-                if (v < mm) lo = mid + 1; else hi = mid - 1;
-            }
-            if (pos >= 0) {
-                U.dst[h] = 3 * pos + (j - 3 * kk);
-                // row q of m owns j when j > 3*msk + q (strictly upper)
-#pragma unroll
-                for (int q = 0; q < 3; ++q)
-                    if (j > 3 * msk + q) U.u[h][q] = ld_cg(urow + (size_t)q * mrl + j);
-            }
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < 3; ++q) U.dinv[q] = ld_cg(dinv + 3 * (size_t)m + q);
-    (void)U.jj;
+__device__ __forceinline__ T pick3(const T v[3], int s) {
+    return s == 0 ? v[0] : s == 1 ? v[1] : v[2];
+}
+template <typename T>
+__device__ __forceinline__ void put3(T v[3], int s, T x) {
+    if (s == 0) v[0] = x;
+    else if (s == 1) v[1] = x;
+    else v[2] = x;
 }
 
 template <typename T>
@@ -100,6 +75,7 @@ __global__ void __launch_bounds__(kNodeWarps * 32)
                  T* __restrict__ dinv, unsigned* __restrict__ done, unsigned epoch,
                  unsigned* __restrict__ status) {
     __shared__ IluStage<T> stage[kNodeWarps];
+    constexpr int UCAP = kUStage / (int)sizeof(T);
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
     IluStage<T>& G = stage[wi];
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -109,85 +85,166 @@ __global__ void __launch_bounds__(kNodeWarps * 32)
         const uint32_t nb0 = __ldg(S.nbr_ptr + n);
         const int deg = (int)(__ldg(S.nbr_ptr + n + 1) - nb0);
         const int sk = (int)__ldg(S.self_pos + n);
-        const int rl = 3 * deg;
+        const int rl = 3 * deg, ds = 3 * sk;
         const T* arow = a + 9 * (size_t)nb0;
-        __syncwarp();
-        for (int i = lane; i < rl; i += 32) {
-            G.w[0][i] = arow[i];
-            G.w[1][i] = arow[rl + i];
-            G.w[2][i] = arow[2 * rl + i];
-        }
+        T w[3][3];
+#pragma unroll
+        for (int p = 0; p < 3; ++p)
+#pragma unroll
+            for (int s = 0; s < 3; ++s) {
+                const int j = lane + 32 * s;
+                w[p][s] = j < rl ? arow[(size_t)p * rl + j] : T(0);
+            }
+        const T adiag = lane < 3 ? arow[(size_t)lane * rl + ds + lane] : T(0);
         const uint32_t my_nbr = lane < deg ? __ldg(S.nbr + nb0 + lane) : 0xffffffffu;
-        G.nbr[lane] = my_nbr;
+        uint32_t mb0 = 0, mdeg = 0, msk = 0;
+        if (lane < sk) {
+            mb0 = __ldg(S.nbr_ptr + my_nbr);
+            mdeg = __ldg(S.nbr_ptr + my_nbr + 1) - mb0;
+            msk = __ldg(S.self_pos + my_nbr);
+        }
+        const uint32_t np = mdeg - msk;  // pairs of lower neighbour `lane` (0 beyond sk)
+        uint32_t incl = np;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const uint32_t eb = __ldg(S.emap_ptr + n);
+        __syncwarp();  // the previous node's reads of G are done
+        G.poff[lane] = incl - np;
+        if (lane == 31) G.poff[32] = incl;
+        G.mb0[lane] = mb0;
+        G.mdeg[lane] = (uint8_t)mdeg;
+        G.msk[lane] = (uint8_t)msk;
         // wait for every lower neighbour node's rows
         bool ok = true;
         if (lane < sk) ok = wait_flag(done + my_nbr, epoch, status);
         ok = __all_sync(kFull, ok);
+        T dv0 = T(0), dv1 = T(0), dv2 = T(0);
+        if (ok && lane < sk) {
+            dv0 = ld_cg(dinv + 3 * (size_t)my_nbr);
+            dv1 = ld_cg(dinv + 3 * (size_t)my_nbr + 1);
+            dv2 = ld_cg(dinv + 3 * (size_t)my_nbr + 2);
+        }
         __syncwarp();
-        if (ok && sk > 0) {
-            URows<T> cur, nxt;
-            load_urows(S, lu, dinv, G.nbr, deg, G.nbr[0], lane, cur);
-            for (int k = 0; k < sk; ++k) {
-                if (k + 1 < sk) load_urows(S, lu, dinv, G.nbr, deg, G.nbr[k + 1], lane, nxt);
+        const int cap_k = UCAP / (3 * rl) > 0 ? UCAP / (3 * rl) : 1;
+        for (int k0 = 0; ok && k0 < sk; k0 += cap_k) {
+            const int k1 = k0 + cap_k < sk ? k0 + cap_k : sk;
+            const int nu = (k1 - k0) * 3 * rl;
+            for (int i = lane; i < nu; i += 32) G.u[i] = T(0);
+            __syncwarp();
+            const uint32_t p0 = G.poff[k0], p1 = G.poff[k1];
+            for (uint32_t base = p0; base < p1; base += 32 * kPairRound) {
+                T val[kPairRound][9];
+                int dst[kPairRound];
+                // loads of a round in flight together
+#pragma unroll
+                for (int r = 0; r < kPairRound; ++r) {
+                    dst[r] = -1;
+                    const uint32_t pr = base + lane + 32 * r;
+                    if (pr < p1) {
+                        int k = k0;
+                        while (k + 1 < k1 && G.poff[k + 1] <= pr) ++k;
+                        const uint32_t pos = __ldg(S.emap + eb + pr);
+                        if (pos != 0xffu) {
+                            const int ms = G.msk[k], mrl = 3 * (int)G.mdeg[k];
+                            const int kk = ms + (int)(pr - G.poff[k]);
+                            const T* urow = lu + 9 * (size_t)G.mb0[k];
+                            dst[r] = ((k - k0) * 3) * rl + 3 * (int)pos;
+#pragma unroll
+                            for (int q = 0; q < 3; ++q)
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) {
+                                    const int j = 3 * kk + c;
+                                    val[r][3 * q + c] =
+                                        j > 3 * ms + q ? ld_cg(urow + (size_t)q * mrl + j) : T(0);
+                                }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < kPairRound; ++r)
+                    if (dst[r] >= 0)
+#pragma unroll
+                        for (int q = 0; q < 3; ++q)
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) G.u[dst[r] + q * rl + c] = val[r][3 * q + c];
+            }
+            __syncwarp();
+            for (int k = k0; k < k1; ++k) {
+                const T dk[3] = {__shfl_sync(kFull, dv0, k), __shfl_sync(kFull, dv1, k),
+                                 __shfl_sync(kFull, dv2, k)};
 #pragma unroll
                 for (int q = 0; q < 3; ++q) {
                     // multipliers of column c = 3m+q in the node's three rows
-                    const T l0 = G.w[0][3 * k + q] * cur.dinv[q];
-                    const T l1 = G.w[1][3 * k + q] * cur.dinv[q];
-                    const T l2 = G.w[2][3 * k + q] * cur.dinv[q];
+                    const int c = 3 * k + q, owner = c & 31, sl = c >> 5;
+                    const T l0 = __shfl_sync(kFull, pick3(w[0], sl), owner) * dk[q];
+                    const T l1 = __shfl_sync(kFull, pick3(w[1], sl), owner) * dk[q];
+                    const T l2 = __shfl_sync(kFull, pick3(w[2], sl), owner) * dk[q];
+                    const T* ur = G.u + ((k - k0) * 3 + q) * rl;
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int d = cur.dst[h];
-                        if (d >= 0 && cur.u[h][q] != T(0)) {
-                            const T uv = cur.u[h][q];
-                            G.w[0][d] -= l0 * uv;
-                            G.w[1][d] -= l1 * uv;
-                            G.w[2][d] -= l2 * uv;
+                    for (int s = 0; s < 3; ++s) {
+                        const int j = lane + 32 * s;
+                        if (j < rl) {
+                            const T uv = ur[j];
+                            if (uv != T(0)) {
+                                w[0][s] -= l0 * uv;
+                                w[1][s] -= l1 * uv;
+                                w[2][s] -= l2 * uv;
+                            }
                         }
                     }
-                    __syncwarp();
-                    if (lane == 0) {
-                        G.w[0][3 * k + q] = l0;
-                        G.w[1][3 * k + q] = l1;
-                        G.w[2][3 * k + q] = l2;
+                    if (lane == owner) {
+                        put3(w[0], sl, l0);
+                        put3(w[1], sl, l1);
+                        put3(w[2], sl, l2);
                     }
-                    __syncwarp();
                 }
-                if (k + 1 < sk) cur = nxt;
             }
+            __syncwarp();  // before the next chunk overwrites G.u
         }
         // the node's own 3x3 block: columns 3n and 3n+1 eliminate rows below
-        const int ds = 3 * sk;
         T piv[3];
+#pragma unroll
         for (int p = 0; p < 3; ++p) {
-            T u = G.w[p][ds + p];
+            const int c = ds + p, owner = c & 31, sl = c >> 5;
+            T u = __shfl_sync(kFull, pick3(w[p], sl), owner);
             if (fabs((double)u) < kPivotThreshold) {
                 u += (u >= T(0) ? T(kPivotPerturb) : T(-kPivotPerturb));
                 if (lane == 0) raise_flag(status, FM_FLAG_PIVOT);
             }
             piv[p] = u;
-            __syncwarp();
+#pragma unroll
             for (int r2 = p + 1; r2 < 3; ++r2) {
-                const T l = G.w[r2][ds + p] / u;
-                for (int j = ds + p + 1 + lane; j < rl; j += 32) G.w[r2][j] -= l * G.w[p][j];
-                __syncwarp();
-                if (lane == 0) G.w[r2][ds + p] = l;
-                __syncwarp();
+                const T l = __shfl_sync(kFull, pick3(w[r2], sl), owner) / u;
+#pragma unroll
+                for (int s = 0; s < 3; ++s) {
+                    const int j = lane + 32 * s;
+                    if (j > c && j < rl) w[r2][s] -= l * w[p][s];
+                }
+                if (lane == owner) put3(w[r2], sl, l);
             }
         }
         // write back: diagonal slots keep a_ii (the pivots go to dg)
         T* out = lu + 9 * (size_t)nb0;
-        for (int i = lane; i < rl; i += 32) {
-            out[i] = (i == ds) ? arow[i] : G.w[0][i];
-            out[rl + i] = (i == ds + 1) ? arow[rl + i] : G.w[1][i];
-            out[2 * rl + i] = (i == ds + 2) ? arow[2 * rl + i] : G.w[2][i];
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+            const T ap = __shfl_sync(kFull, adiag, p);
+#pragma unroll
+            for (int s = 0; s < 3; ++s) {
+                const int j = lane + 32 * s;
+                if (j < rl) out[(size_t)p * rl + j] = (j == ds + p) ? ap : w[p][s];
+            }
         }
         if (lane < 3) {
-            dg[3 * (size_t)n + lane] = piv[lane];
-            dinv[3 * (size_t)n + lane] = T(1) / piv[lane];
-            if (!isfinite((double)piv[lane])) raise_flag(status, FM_FLAG_NONFINITE);
+            const T pv = pick3(piv, lane);
+            dg[3 * (size_t)n + lane] = pv;
+            dinv[3 * (size_t)n + lane] = T(1) / pv;
+            if (!isfinite((double)pv)) raise_flag(status, FM_FLAG_NONFINITE);
         }
-        __threadfence();
+        // the warp barrier orders every lane's row writes before lane 0's
+        // release store (release is cumulative)
         __syncwarp();
         if (lane == 0) st_release(done + n, epoch);
     }

@@ -21,6 +21,9 @@ struct NodeSched {
     const uint4* fwd_rec = nullptr;
     const uint4* bwd_rec = nullptr;
     uint32_t max_width_fwd = 0, max_width_bwd = 0;
+    // ILU(0) update map (fm_setup.cpp ilu_edge_maps): per node offset, entries
+    const uint32_t* emap_ptr = nullptr;
+    const uint8_t* emap = nullptr;
 };
 
 // y = U^-1 L^-1 r using tmp for the intermediate (both overwritten);
@@ -34,5 +37,39 @@ void launch_ilu0_nodes(const NodeSched& S, const T* a, T* lu, T* d, T* dinv, uns
                        unsigned epoch, unsigned* status, int device, cudaStream_t s);
 template <typename T>
 void launch_fill_sentinel(uint32_t n, T* x, cudaStream_t s);
+
+// One direction of the cluster-synchronous solves (fm_trsv_cluster.cu):
+// the level pointers, per-position records {node, first neighbour entry,
+// deg | sk << 8 | cnt << 16, own slot} and per-neighbour-entry slots
+// (cta << 16 | index) of fm_setup.cpp cluster_plan, on the device.
+struct ClusterSolve {
+    uint32_t n_levels = 0, n_ctas = 0, warps_per_cta = 0;
+    uint32_t max_per_warp = 0;  // nodes of one level per warp, at most (<= 32)
+    uint32_t maxc = 0;          // neighbours on the solve's side, at most (<= 32)
+    uint32_t pool_slots = 0;    // value slots per CTA (16 bytes each in FP32, 32 in FP64)
+    uint32_t window = 1;        // levels between cluster barriers
+    const uint32_t* lvl_ptr = nullptr;
+    const uint4* rec = nullptr;
+    const uint32_t* nslot = nullptr;
+    const uint32_t* reset_ptr = nullptr;  // per (window, CTA): slots to reset after it
+    const uint32_t* reset = nullptr;
+};
+// bytes of one packed card, dynamic shared memory of one CTA, stage depth
+size_t cluster_card_bytes(const ClusterSolve& P, size_t value_bytes);
+size_t cluster_smem_bytes(const ClusterSolve& P, size_t value_bytes, int stages);
+int cluster_stages(size_t value_bytes);
+// clusters of cs CTAs (one per SM, 1024 threads, smem bytes each) that can be
+// resident at once for the solve kernels of this value width (0: none)
+int cluster_max_active(size_t value_bytes, int cs, size_t smem);
+// pack the factors into both directions' cards (after each factorization)
+template <typename T>
+void launch_pack_cards(const ClusterSolve& F, const ClusterSolve& B, const uint32_t* card_f,
+                       const uint32_t* card_b, uint32_t n_pos, const T* lu, const T* dinv,
+                       unsigned char* packed_f, unsigned char* packed_b, cudaStream_t s);
+// y = U^-1 L^-1 r through tmp from the packed cards
+template <typename T>
+cudaError_t launch_trsv_cluster(const ClusterSolve& F, const ClusterSolve& B,
+                                const unsigned char* packed_f, const unsigned char* packed_b,
+                                const T* r, T* tmp, T* y, unsigned* status, cudaStream_t s);
 
 }  // namespace fm
