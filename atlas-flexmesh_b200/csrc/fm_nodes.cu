@@ -13,6 +13,8 @@
 // and all waits end.  The factorization, whose outputs are whole rows,
 // releases a per-node flag; the triangular solves (fm_trsv.cu) wait on the
 // dependencies' values directly.
+#include <cstdlib>
+
 #include "fm_kernels.hpp"
 #include "fm_nodes.hpp"
 #include "fm_sync.cuh"
@@ -73,7 +75,7 @@ template <typename T>
 __global__ void __launch_bounds__(kNodeWarps * 32)
     k_ilu0_nodes(NodeSched S, const T* __restrict__ a, T* __restrict__ lu, T* __restrict__ dg,
                  T* __restrict__ dinv, unsigned* __restrict__ done, unsigned epoch,
-                 unsigned* __restrict__ status) {
+                 unsigned* __restrict__ status, unsigned sleep_ns) {
     __shared__ IluStage<T> stage[kNodeWarps];
     constexpr int UCAP = kUStage / (int)sizeof(T);
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
@@ -118,9 +120,8 @@ __global__ void __launch_bounds__(kNodeWarps * 32)
         G.mdeg[lane] = (uint8_t)mdeg;
         G.msk[lane] = (uint8_t)msk;
         // wait for every lower neighbour node's rows
-        bool ok = true;
-        if (lane < sk) ok = wait_flag(done + my_nbr, epoch, status);
-        ok = __all_sync(kFull, ok);
+        const bool ok = wait_flags_warp(done + (lane < sk ? my_nbr : 0), lane < sk, epoch,
+                                        status, sleep_ns);
         T dv0 = T(0), dv1 = T(0), dv2 = T(0);
         if (ok && lane < sk) {
             dv0 = ld_cg(dinv + 3 * (size_t)my_nbr);
@@ -182,23 +183,17 @@ __global__ void __launch_bounds__(kNodeWarps * 32)
                     const T l0 = __shfl_sync(kFull, pick3(w[0], sl), owner) * dk[q];
                     const T l1 = __shfl_sync(kFull, pick3(w[1], sl), owner) * dk[q];
                     const T l2 = __shfl_sync(kFull, pick3(w[2], sl), owner) * dk[q];
+                    // branch-free: the warp stays converged for the next shuffles
                     const T* ur = G.u + ((k - k0) * 3 + q) * rl;
 #pragma unroll
                     for (int s = 0; s < 3; ++s) {
                         const int j = lane + 32 * s;
-                        if (j < rl) {
-                            const T uv = ur[j];
-                            if (uv != T(0)) {
-                                w[0][s] -= l0 * uv;
-                                w[1][s] -= l1 * uv;
-                                w[2][s] -= l2 * uv;
-                            }
-                        }
-                    }
-                    if (lane == owner) {
-                        put3(w[0], sl, l0);
-                        put3(w[1], sl, l1);
-                        put3(w[2], sl, l2);
+                        const T uv = ur[j < rl ? j : rl - 1];
+                        const bool upd = j < rl && uv != T(0);
+                        const bool own = lane == owner && s == sl;
+                        w[0][s] = own ? l0 : upd ? w[0][s] - l0 * uv : w[0][s];
+                        w[1][s] = own ? l1 : upd ? w[1][s] - l1 * uv : w[1][s];
+                        w[2][s] = own ? l2 : upd ? w[2][s] - l2 * uv : w[2][s];
                     }
                 }
             }
@@ -221,9 +216,9 @@ __global__ void __launch_bounds__(kNodeWarps * 32)
 #pragma unroll
                 for (int s = 0; s < 3; ++s) {
                     const int j = lane + 32 * s;
-                    if (j > c && j < rl) w[r2][s] -= l * w[p][s];
+                    const bool own = lane == owner && s == sl;
+                    w[r2][s] = own ? l : (j > c && j < rl) ? w[r2][s] - l * w[p][s] : w[r2][s];
                 }
-                if (lane == owner) put3(w[r2], sl, l);
             }
         }
         // write back: diagonal slots keep a_ii (the pivots go to dg)
@@ -279,8 +274,13 @@ void launch_ilu0_nodes(const NodeSched& S, const T* a, T* lu, T* d, T* dinv, uns
     static int res[2] = {0, 0};
     const int f = sizeof(T) == 4;
     if (!res[f]) res[f] = resident_grid_nodes(k_ilu0_nodes<T>, device);
+    // FM_ILU_SLEEP_NS: longest sleep between a waiting warp's polls
+    static const unsigned sleep_ns = [] {
+        const char* v = getenv("FM_ILU_SLEEP_NS");
+        return v ? (unsigned)strtoul(v, nullptr, 10) : 0u;
+    }();
     k_ilu0_nodes<T><<<grid_for(res[f], S.max_width_fwd), kNodeWarps * 32, 0, s>>>(
-        S, a, lu, d, dinv, done, epoch, status);
+        S, a, lu, d, dinv, done, epoch, status, sleep_ns);
 }
 
 template void launch_ilu0_nodes<double>(const NodeSched&, const double*, double*, double*,

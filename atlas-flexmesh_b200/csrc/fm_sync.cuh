@@ -96,4 +96,43 @@ __device__ __forceinline__ void wait_values3(const T* p, unsigned* status, T& v0
     }
 }
 
+// Warp-uniform form of wait_values3: lanes with p != nullptr wait for their
+// node's three values, and all lanes leave together (warp vote), so the
+// warp stays converged for the reduction that follows.  After 16 polls the
+// loop sleeps between polls, doubling from 32 ns up to sleep_ns (0: never).
+template <typename T>
+__device__ __forceinline__ void wait_values3_warp(const T* p, unsigned* status, unsigned sleep_ns,
+                                                  T& v0, T& v1, T& v2) {
+    bool need = p != nullptr;
+    v0 = v1 = v2 = T(0);
+    if (need) {
+        v0 = ld_relaxed(p);
+        v1 = ld_relaxed(p + 1);
+        v2 = ld_relaxed(p + 2);
+        need = Sentinel<T>::is(v0) | Sentinel<T>::is(v1) | Sentinel<T>::is(v2);
+    }
+    if (!__any_sync(kFull, need)) return;
+    const long long t0 = clock64();
+    unsigned ns = 32;
+    for (unsigned it = 1;; ++it) {
+        if (sleep_ns && it > 16) {
+            __nanosleep(ns);
+            if (ns < sleep_ns) ns <<= 1;
+        }
+        if (need) {
+            if (Sentinel<T>::is(v0)) v0 = ld_relaxed(p);
+            if (Sentinel<T>::is(v1)) v1 = ld_relaxed(p + 1);
+            if (Sentinel<T>::is(v2)) v2 = ld_relaxed(p + 2);
+            need = Sentinel<T>::is(v0) | Sentinel<T>::is(v1) | Sentinel<T>::is(v2);
+        }
+        if (!__any_sync(kFull, need)) return;
+        if ((it & 63u) == 0 &&
+            __any_sync(kFull, (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) ||
+                                  clock64() - t0 > kWaitCycles)) {
+            if ((threadIdx.x & 31) == 0) raise_flag(status, FM_FLAG_TIMEOUT);
+            return;
+        }
+    }
+}
+
 }  // namespace fm

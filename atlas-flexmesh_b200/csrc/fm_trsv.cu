@@ -13,11 +13,11 @@
 //
 // Lane k of the warp owns neighbour node k of the solve's side (lower
 // neighbours for L, upper ones for U): it waits for that node's three
-// values and forms the 3x3 block product, so the row sums gather at most
-// one partial per neighbour (<= 9 on the unit cube).  The gather goes
-// through shared memory: on B200 three FP64 shuffle trees after the lanes'
-// divergent waits measured ~4 us per node against ~0.8 us for a shared
-// gather, on the critical path of every level.
+// values and forms the 3x3 block product; a butterfly sums the partials.
+// The waits run in lock step (the loop's exit is a warp vote): lanes that
+// spin separately split the warp, and on B200 its reconvergence before the
+// reduction cost more than the dependency hop itself (traced per node with
+// %globaltimer: 1.23 -> 0.73 ms per FP32 forward+backward pair at 64^3).
 #include <cstdlib>
 
 #include "fm_kernels.hpp"
@@ -103,28 +103,27 @@ __device__ __forceinline__ void pre_upper(const NodeSched& S, uint4 rec, const T
     }
 }
 
-// Row sums sum_k A_k v_k of the node (valid in lane 0).
+// Row sums sum_k A_k v_k of the node (valid in every lane).  The waits run
+// in lock step (warp-uniform exit), so the butterfly that follows starts on
+// a converged warp.
 template <typename T>
 __device__ __forceinline__ void block_sums(const TrsvPre<T>& P, unsigned* status,
-                                           unsigned backoff, T (*red)[32], int lane, T& s0,
-                                           T& s1, T& s2) {
-    (void)backoff;
-    if (P.vp) {
-        T v0, v1, v2;
-        wait_values3(P.vp, status, v0, v1, v2);
-        red[0][lane] = P.a[0] * v0 + P.a[1] * v1 + P.a[2] * v2;
-        red[1][lane] = P.a[3] * v0 + P.a[4] * v1 + P.a[5] * v2;
-        red[2][lane] = P.a[6] * v0 + P.a[7] * v1 + P.a[8] * v2;
-    }
-    __syncwarp();
+                                           unsigned sleep_ns, int lane, T& s0, T& s1, T& s2) {
+    (void)lane;
+    T v0, v1, v2;
+    wait_values3_warp(P.vp, status, sleep_ns, v0, v1, v2);
     s0 = s1 = s2 = T(0);
-    if (lane == 0)
-        for (int i = 0; i < P.cnt; ++i) {
-            s0 += red[0][i];
-            s1 += red[1][i];
-            s2 += red[2][i];
-        }
-    __syncwarp();
+    if (P.vp) {
+        s0 = P.a[0] * v0 + P.a[1] * v1 + P.a[2] * v2;
+        s1 = P.a[3] * v0 + P.a[4] * v1 + P.a[5] * v2;
+        s2 = P.a[6] * v0 + P.a[7] * v1 + P.a[8] * v2;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        s0 += __shfl_xor_sync(kFull, s0, o);
+        s1 += __shfl_xor_sync(kFull, s1, o);
+        s2 += __shfl_xor_sync(kFull, s2, o);
+    }
 }
 
 // z = L^-1 r, L unit lower (per node: z0, then z1 and z2 with the own block)
@@ -132,7 +131,6 @@ template <typename T>
 __global__ void __launch_bounds__(kTrsvWarps * 32)
     k_trsv_lower_pipe(NodeSched S, const T* __restrict__ lu, const T* __restrict__ r,
                       T* __restrict__ z, unsigned* __restrict__ status, unsigned backoff) {
-    __shared__ T red[kTrsvWarps][3][32];
     const int lane = threadIdx.x & 31;
     const uint32_t W = (gridDim.x * blockDim.x) >> 5;
     uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -145,7 +143,7 @@ __global__ void __launch_bounds__(kTrsvWarps * 32)
         if (more) pre_lower(S, rec_n, lu, r, z, lane, nxt);
         if (t + 2 * W < S.n_nodes) rec_n = __ldg(S.fwd_rec + t + 2 * W);
         T s0, s1, s2;
-        block_sums(cur, status, backoff, red[threadIdx.x >> 5], lane, s0, s1, s2);
+        block_sums(cur, status, backoff, lane, s0, s1, s2);
         if (lane == 0) {
             const T z0 = cur.c[0] - s0;
             const T z1 = cur.c[1] - s1 - cur.c[3] * z0;
@@ -167,7 +165,6 @@ __global__ void __launch_bounds__(kTrsvWarps * 32)
     k_trsv_upper_pipe(NodeSched S, const T* __restrict__ lu, const T* __restrict__ dinv,
                       const T* __restrict__ zin, T* __restrict__ y, unsigned* __restrict__ status,
                       unsigned backoff) {
-    __shared__ T red[kTrsvWarps][3][32];
     const int lane = threadIdx.x & 31;
     const uint32_t W = (gridDim.x * blockDim.x) >> 5;
     uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -180,7 +177,7 @@ __global__ void __launch_bounds__(kTrsvWarps * 32)
         if (more) pre_upper(S, rec_n, lu, dinv, zin, y, lane, nxt);
         if (t + 2 * W < S.n_nodes) rec_n = __ldg(S.bwd_rec + t + 2 * W);
         T s0, s1, s2;
-        block_sums(cur, status, backoff, red[threadIdx.x >> 5], lane, s0, s1, s2);
+        block_sums(cur, status, backoff, lane, s0, s1, s2);
         if (lane == 0) {
             const T y2 = (cur.c[2] - s2) * cur.s[2];
             const T y1 = (cur.c[1] - s1 - cur.c[5] * y2) * cur.s[1];
@@ -207,8 +204,8 @@ static int resident_grid_trsv(K kernel, int device) {
 
 // Tuning (environment, read once): FM_TRSV_WARPS_PER_WIDTH = warps per 16
 // nodes of the widest dependency level (default 24, i.e. 1.5x);
-// FM_TRSV_BACKOFF_NS = first poll back-off (default 0: plain spinning
-// measured fastest).  The grid never exceeds what can be resident at once:
+// FM_TRSV_BACKOFF_NS = longest sleep between a waiting warp's polls
+// (default 0: plain spinning).  The grid never exceeds what can be resident at once:
 // every warp must run for the waits to end.
 static unsigned env_u(const char* name, unsigned dflt) {
     const char* v = getenv(name);

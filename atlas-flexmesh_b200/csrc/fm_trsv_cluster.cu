@@ -153,25 +153,6 @@ __device__ __forceinline__ void st_slot(uint32_t addr, T a, T b, T c) {
     st_val(addr + sizeof(T), b);
     st_val(addr + 2 * sizeof(T), c);
 }
-// Bounded poll of a slot (remote or local); false when the wait gave up.
-template <typename T>
-__device__ __forceinline__ bool poll_slot(uint32_t addr, T& a, T& b, T& c, unsigned* status) {
-    ld_slot<T>(addr, a, b, c);
-    if (!(Sentinel<T>::is(a) | Sentinel<T>::is(b) | Sentinel<T>::is(c))) return true;
-    const long long t0 = clock64();
-    for (unsigned it = 1;; ++it) {
-        ld_slot<T>(addr, a, b, c);
-        if (!(Sentinel<T>::is(a) | Sentinel<T>::is(b) | Sentinel<T>::is(c))) return true;
-        if ((it & 63u) == 0) {
-            if (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) return false;
-            if (clock64() - t0 > kWaitCycles) {
-                raise_flag(status, FM_FLAG_TIMEOUT);
-                return false;
-            }
-        }
-    }
-}
-
 // Packed card of one node (byte offsets; 16-byte multiple):
 //   [0,16)    schedule record {node, first entry, deg | sk<<8 | cnt<<16, own slot}
 //   h[6]      forward: L(1,0) L(2,0) L(2,1), unused(3)
@@ -325,25 +306,61 @@ __global__ void __launch_bounds__(1024, 1)
         const unsigned char* st = my + s * stage_bytes;
         const T* rh = reinterpret_cast<const T*>(st + cards_bytes);
         for (uint32_t j0 = 0; j0 < m; j0 += kChunk) {
-            T part[kChunk][3];
+            // the chunk's dependency values: lane k polls neighbour k of each
+            // node; the loop runs in lock step (its exit is warp-uniform), so
+            // the warp never splits into separately spinning lanes, whose
+            // reconvergence before the shuffles costs microseconds
+            T v[kChunk][3];
+            uint32_t addr[kChunk];
+            bool need[kChunk];
 #pragma unroll
             for (int c = 0; c < kChunk; ++c) {
-                part[c][0] = part[c][1] = part[c][2] = T(0);
                 const uint32_t j = j0 + c;
+                need[c] = false;
+                addr[c] = 0;
                 if (j < m) {
                     const unsigned char* cd = st + j * card;
                     const uint32_t cnt = reinterpret_cast<const uint4*>(cd)->z >> 16;
                     if ((uint32_t)lane < cnt) {
                         const uint32_t sl =
                             reinterpret_cast<const uint32_t*>(cd + Card<T>::s_off(P.maxc))[lane];
-                        T v0, v1, v2;
-                        poll_slot<T>(mapa(pool_sa + (sl & 0xffffu) * VS, sl >> 16), v0, v1, v2,
-                                     status);
-                        const T* a = reinterpret_cast<const T*>(cd + Card<T>::a_off()) + 9 * lane;
-                        part[c][0] = a[0] * v0 + a[1] * v1 + a[2] * v2;
-                        part[c][1] = a[3] * v0 + a[4] * v1 + a[5] * v2;
-                        part[c][2] = a[6] * v0 + a[7] * v1 + a[8] * v2;
+                        addr[c] = mapa(pool_sa + (sl & 0xffffu) * VS, sl >> 16);
+                        need[c] = true;
                     }
+                }
+                v[c][0] = v[c][1] = v[c][2] = T(0);
+            }
+            const long long t0 = clock64();
+            for (unsigned it = 0;; ++it) {
+                bool ready = true;
+#pragma unroll
+                for (int c = 0; c < kChunk; ++c)
+                    if (need[c]) {
+                        ld_slot<T>(addr[c], v[c][0], v[c][1], v[c][2]);
+                        need[c] = Sentinel<T>::is(v[c][0]) | Sentinel<T>::is(v[c][1]) |
+                                  Sentinel<T>::is(v[c][2]);
+                        ready &= !need[c];
+                    }
+                if (__all_sync(0xffffffffu, ready)) break;
+                if ((it & 63u) == 63u &&
+                    __any_sync(0xffffffffu, (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) ||
+                                                clock64() - t0 > kWaitCycles)) {
+                    if (lane == 0) raise_flag(status, FM_FLAG_TIMEOUT);
+                    break;
+                }
+            }
+            T part[kChunk][3];
+#pragma unroll
+            for (int c = 0; c < kChunk; ++c) {
+                const uint32_t j = j0 + c;
+                part[c][0] = part[c][1] = part[c][2] = T(0);
+                const unsigned char* cd = st + (j < m ? j : 0) * card;
+                const uint32_t cnt = j < m ? reinterpret_cast<const uint4*>(cd)->z >> 16 : 0;
+                if ((uint32_t)lane < cnt) {
+                    const T* a = reinterpret_cast<const T*>(cd + Card<T>::a_off()) + 9 * lane;
+                    part[c][0] = a[0] * v[c][0] + a[1] * v[c][1] + a[2] * v[c][2];
+                    part[c][1] = a[3] * v[c][0] + a[4] * v[c][1] + a[5] * v[c][2];
+                    part[c][2] = a[6] * v[c][0] + a[7] * v[c][1] + a[8] * v[c][2];
                 }
             }
 #pragma unroll
