@@ -173,27 +173,51 @@ __global__ void __launch_bounds__(kNodeWarps * 32)
                             for (int c = 0; c < 3; ++c) G.u[dst[r] + q * rl + c] = val[r][3 * q + c];
             }
             __syncwarp();
+            const int nsl = (rl + 31) >> 5;  // column slots in use (warp-uniform)
             for (int k = k0; k < k1; ++k) {
-                const T dk[3] = {__shfl_sync(kFull, dv0, k), __shfl_sync(kFull, dv1, k),
-                                 __shfl_sync(kFull, dv2, k)};
+                // the three pivot columns c_q = 3k + q of neighbour m = nbr[k]:
+                // multipliers by forward substitution through m's own U block
+                // (the reference's column order, zero entries skipped), then one
+                // pass over the owned columns subtracts l_0 U_0j, l_1 U_1j and
+                // l_2 U_2j in that order
+                const T d0 = __shfl_sync(kFull, dv0, k), d1 = __shfl_sync(kFull, dv1, k),
+                        d2 = __shfl_sync(kFull, dv2, k);
+                const T* ur0 = G.u + ((k - k0) * 3 + 0) * rl;
+                const T* ur1 = ur0 + rl;
+                const T* ur2 = ur1 + rl;
+                const int c0 = 3 * k;
+                const T u01 = ur0[c0 + 1], u02 = ur0[c0 + 2], u12 = ur1[c0 + 2];
+                T l[3][3];  // l[p][q]
 #pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    // multipliers of column c = 3m+q in the node's three rows
-                    const int c = 3 * k + q, owner = c & 31, sl = c >> 5;
-                    const T l0 = __shfl_sync(kFull, pick3(w[0], sl), owner) * dk[q];
-                    const T l1 = __shfl_sync(kFull, pick3(w[1], sl), owner) * dk[q];
-                    const T l2 = __shfl_sync(kFull, pick3(w[2], sl), owner) * dk[q];
-                    // branch-free: the warp stays converged for the next shuffles
-                    const T* ur = G.u + ((k - k0) * 3 + q) * rl;
+                for (int p = 0; p < 3; ++p) {
+                    T wq[3];
 #pragma unroll
-                    for (int s = 0; s < 3; ++s) {
+                    for (int q = 0; q < 3; ++q)
+                        wq[q] = __shfl_sync(kFull, pick3(w[p], (c0 + q) >> 5), (c0 + q) & 31);
+                    l[p][0] = wq[0] * d0;
+                    const T t1 = u01 != T(0) ? wq[1] - l[p][0] * u01 : wq[1];
+                    l[p][1] = t1 * d1;
+                    T t2 = u02 != T(0) ? wq[2] - l[p][0] * u02 : wq[2];
+                    t2 = u12 != T(0) ? t2 - l[p][1] * u12 : t2;
+                    l[p][2] = t2 * d2;
+                }
+#pragma unroll
+                for (int s = 0; s < 3; ++s) {
+                    if (s < nsl) {
                         const int j = lane + 32 * s;
-                        const T uv = ur[j < rl ? j : rl - 1];
-                        const bool upd = j < rl && uv != T(0);
-                        const bool own = lane == owner && s == sl;
-                        w[0][s] = own ? l0 : upd ? w[0][s] - l0 * uv : w[0][s];
-                        w[1][s] = own ? l1 : upd ? w[1][s] - l1 * uv : w[1][s];
-                        w[2][s] = own ? l2 : upd ? w[2][s] - l2 * uv : w[2][s];
+                        const int jc = j < rl ? j : rl - 1;
+                        const T a0 = ur0[jc], a1 = ur1[jc], a2 = ur2[jc];
+                        const bool in = j < rl;
+#pragma unroll
+                        for (int p = 0; p < 3; ++p) {
+                            T x = w[p][s];
+                            x = in && a0 != T(0) ? x - l[p][0] * a0 : x;
+                            x = in && a1 != T(0) ? x - l[p][1] * a1 : x;
+                            x = in && a2 != T(0) ? x - l[p][2] * a2 : x;
+                            // the pivot columns take their multipliers
+                            x = j == c0 ? l[p][0] : j == c0 + 1 ? l[p][1] : j == c0 + 2 ? l[p][2] : x;
+                            w[p][s] = x;
+                        }
                     }
                 }
             }

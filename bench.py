@@ -118,6 +118,21 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def profiled_traffic(key):
+    """DRAM bytes per call of one kernel class, measured by ncu on this
+    workload and recorded in the committed summaries under profiles/ as
+    'machine-readable: traffic_bytes_per_call <key> <bytes>' (None if absent)"""
+    import glob
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        with open(path) as f:
+            for line in f:
+                parts = line.split()
+                if (len(parts) == 4 and parts[0] == "machine-readable:" and
+                        parts[1] == "traffic_bytes_per_call" and parts[2] == key):
+                    return int(parts[3])
+    return None
+
+
 def trsv_bytes(nnz, n, w, wv):
     """algorithmic bytes of one preconditioner apply (forward + backward)"""
     return (w + 4) * (nnz - n) + w * n + 8 * (n + 1) + 4 * wv * n
@@ -237,7 +252,8 @@ def run_flexmesh(args, rank, world, local, dist):
         avg_s = prof[dom]["ms"] / 1e3 / prof[dom]["calls"]
         ach = per[dom] / avg_s / 1e9
         roof = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm,
-                "unit": "GB/s", "frac": round(ach / hbm, 4), "traffic": None,
+                "unit": "GB/s", "frac": round(ach / hbm, 4),
+                "traffic": profiled_traffic(f"{dom}_mixed_n{args.N}"),
                 "peak_kind": peak_kind, "bytes_per_launch": per[dom],
                 "avg_launch_ms": round(avg_s * 1e3, 4)}
     value = E * newton * world / t
