@@ -83,27 +83,17 @@ __device__ __forceinline__ bool wait_flag(const unsigned* flag, unsigned epoch,
     }
 }
 
-__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
 // Warp-uniform bounded wait: every lane with `need` waits for *flag ==
-// epoch; all lanes leave together (the exit test is a warp vote), so the
-// warp never splits into separately spinning lanes.  Polls are relaxed;
-// one acquire fence follows.  After 16 polls the loop sleeps between polls,
-// doubling from 32 ns up to sleep_ns (0: never sleeps), so that warps that
-// wait long leave issue slots to the warps doing the work.  Returns false
-// (FM_FLAG_TIMEOUT set) when the wait exceeds kWaitCycles or another wait
-// already timed out.
+// epoch (acquire loads); all lanes leave together (the exit test is a warp
+// vote), so the warp never splits into separately spinning lanes.  A
+// caller's __syncwarp after it extends each lane's acquire to the whole
+// warp.  After 16 polls the loop sleeps between polls, doubling from 32 ns
+// up to sleep_ns (0: never sleeps).  Returns false (FM_FLAG_TIMEOUT set)
+// when the wait exceeds kWaitCycles or another wait already timed out.
 __device__ __forceinline__ bool wait_flags_warp(const unsigned* flag, bool need, unsigned epoch,
                                                 unsigned* status, unsigned sleep_ns) {
-    bool ok = !need || ld_relaxed_u32(flag) == epoch;
-    if (__all_sync(kFull, ok)) {
-        asm volatile("fence.acq_rel.gpu;" ::: "memory");
-        return true;
-    }
+    bool ok = !need || ld_acquire(flag) == epoch;
+    if (__all_sync(kFull, ok)) return true;
     const long long t0 = clock64();
     unsigned ns = 32;
     for (unsigned it = 1;; ++it) {
@@ -111,11 +101,8 @@ __device__ __forceinline__ bool wait_flags_warp(const unsigned* flag, bool need,
             __nanosleep(ns);
             if (ns < sleep_ns) ns <<= 1;
         }
-        if (!ok) ok = ld_relaxed_u32(flag) == epoch;
-        if (__all_sync(kFull, ok)) {
-            asm volatile("fence.acq_rel.gpu;" ::: "memory");
-            return true;
-        }
+        if (!ok) ok = ld_acquire(flag) == epoch;
+        if (__all_sync(kFull, ok)) return true;
         if ((it & 31u) == 0 &&
             __any_sync(kFull, (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) ||
                                   clock64() - t0 > kWaitCycles)) {

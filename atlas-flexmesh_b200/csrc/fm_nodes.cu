@@ -198,8 +198,9 @@ __global__ void __launch_bounds__(kNodeWarps * 32)
                     dst[r] = -1;
                     const uint32_t pr = base + lane + 32 * r;
                     if (pr < p1) {
+                        // neighbour of this pair: independent compares, not a chain
                         int k = k0;
-                        while (k + 1 < k1 && G.poff[k + 1] <= pr) ++k;
+                        for (int kk = k0 + 1; kk < k1; ++kk) k += (int)(G.poff[kk] <= pr);
                         const uint32_t pos = __ldg(S.emap + eb + pr);
                         if (pos != 0xffu) {
                             const int ms = G.msk[k], mrl = 3 * (int)G.mdeg[k];
