@@ -127,6 +127,7 @@ struct fm_ctx {
     // reference-pattern assembly
     DevBuf<int32_t> ref_slot;
     DevBuf<double> ke_scratch;
+    DevBuf<unsigned char> elem_rec;  // assembly element-pass records
 
     // solver state
     Work<double> w64;
@@ -288,6 +289,7 @@ fm::MeshDev mesh_view(const fm_ctx* c) {
     m.c_mu = c->c_mu;
     m.c_lam = c->c_lam;
     m.inv_cnu = c->inv_cnu;
+    m.elem_rec = c->elem_rec.p;
     return m;
 }
 
@@ -801,6 +803,7 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
         c->ref_slot.release();
         CK(c->vec_a.reserve(c->n));
         CK(c->vec_b.reserve(c->n));
+        CK(c->elem_rec.reserve(std::max<size_t>(1, (size_t)c->ne * fm::kElemRecBytes)));
         CK(cudaStreamSynchronize(c->stream));
     } catch (const std::bad_alloc&) {
         return fail(c, FM_ERR_OOM, "host allocation failed in fm_set_mesh");

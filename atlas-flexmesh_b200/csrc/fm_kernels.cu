@@ -57,11 +57,108 @@ __device__ __forceinline__ int byte_index(uint32_t packed, uint32_t key) {
     return -1;
 }
 
+// Element record (AoS, 16-byte multiple): vertex forces vol M dN_a (FP64,
+// 4x3), shape gradients dN_a (4x3) and tangent scalars vol a, vol b, vol mu
+// in the tangent's type, and an activity mark (0: skipped or degenerate).
+template <typename KT>
+struct ElemRec;
+template <>
+struct __align__(16) ElemRec<double> {
+    double f[12];
+    double d[12];
+    double s[3];
+    double active;
+};
+template <>
+struct __align__(16) ElemRec<float> {
+    double f[12];
+    float d[12];
+    float s[3];
+    float active;
+};
+static_assert(sizeof(ElemRec<double>) <= kElemRecBytes && sizeof(ElemRec<double>) % 16 == 0, "");
+static_assert(sizeof(ElemRec<float>) <= kElemRecBytes && sizeof(ElemRec<float>) % 16 == 0, "");
+
+// Element pass: one thread per tet.  with_k = 0 (residual only) skips the
+// tangent scalars and gradients.
+template <typename KT>
+__global__ void __launch_bounds__(128, 4)
+    k_asm_elements(MeshDev m, const double* __restrict__ u, ElemRec<KT>* __restrict__ rec,
+                   int with_k, unsigned* __restrict__ status) {
+    unsigned flags = 0;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m.n_elems;
+         e += gridDim.x * blockDim.x) {
+        uint4 c = m.conn[e];
+        const bool active = !(c.x & 0x80000000u);
+        c.x &= 0x7fffffffu;
+        const uint32_t cn[4] = {c.x, c.y, c.z, c.w};
+        ElemRec<KT> r;
+#pragma unroll
+        for (int i = 0; i < 12; ++i) {
+            r.f[i] = 0.0;
+            r.d[i] = KT(0);
+        }
+        r.s[0] = r.s[1] = r.s[2] = KT(0);
+        r.active = KT(0);
+        if (active) {
+            double x[12], ue[12];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    x[3 * a + d] = __ldg(m.xyz + 3 * (size_t)cn[a] + d);
+                    ue[3 * a + d] = __ldg(u + 3 * (size_t)cn[a] + d);
+                }
+            TetKin k;
+            if (tet_kinematics(x, ue, k)) {
+                double mu, lam;
+                material_of(m.mat_mode, m.m0, m.m1, e, m.mu_s, m.lam_s, m.c_mu, m.c_lam, mu, lam);
+                const Mandel M = mandel_stress(k.F, k.J, mu, lam);
+                double fs = 0.0;
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    const double* dI = k.d[a];
+                    r.f[3 * a + 0] = k.vol * (M.m00 * dI[0] + M.m01 * dI[1] + M.m02 * dI[2]);
+                    r.f[3 * a + 1] = k.vol * (M.m01 * dI[0] + M.m11 * dI[1] + M.m12 * dI[2]);
+                    r.f[3 * a + 2] = k.vol * (M.m02 * dI[0] + M.m12 * dI[1] + M.m22 * dI[2]);
+                    fs += r.f[3 * a] + r.f[3 * a + 1] + r.f[3 * a + 2];
+                }
+                if (!(k.J > 0.0)) flags |= FM_FLAG_INVERTED;
+                if (k.J < kJSafe) flags |= FM_FLAG_J_CLAMPED;
+                if (!isfinite(fs)) flags |= FM_FLAG_NONFINITE;
+                if (with_k) {
+                    double a, b;
+                    tangent_ab(mu, lam, k.J, M.lnJ, m.inv_cnu, a, b);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) r.d[3 * q + d] = (KT)k.d[q][d];
+                    r.s[0] = (KT)(k.vol * a);
+                    r.s[1] = (KT)(k.vol * b);
+                    r.s[2] = (KT)(k.vol * mu);
+                    if (!isfinite(a + b)) flags |= FM_FLAG_NONFINITE;
+                }
+                r.active = KT(1);
+            }
+        }
+        // 16-byte stores of the whole record
+        const float4* src = reinterpret_cast<const float4*>(&r);
+        float4* dst = reinterpret_cast<float4*>(rec + e);
+#pragma unroll
+        for (int i = 0; i < (int)(sizeof(ElemRec<KT>) / 16); ++i) dst[i] = src[i];
+    }
+    if (flags) raise_flag(status, flags);
+}
+
+// Node pass: one warp owns one node.  Lane l < mi stages incident tet l's
+// record (gradients, the owner's vertex force, tangent scalars) in shared
+// memory; lane k then forms block (n, nbr[k]).
 template <typename KT>
 __global__ void __launch_bounds__(kAsmWarps * 32, 3)
-    k_assemble(MeshDev m, const double* __restrict__ u, KT* __restrict__ K,
+    k_assemble(MeshDev m, const ElemRec<KT>* __restrict__ rec, KT* __restrict__ K,
                double* __restrict__ f, double* __restrict__ R, int apply_bc,
                unsigned* __restrict__ status) {
+    (void)status;
     __shared__ AsmStage<KT> stage[kAsmWarps];
     const int lane = threadIdx.x & 31;
     const int wi = threadIdx.x >> 5;
@@ -80,60 +177,34 @@ __global__ void __launch_bounds__(kAsmWarps * 32, 3)
     __syncwarp();
 
     double fi0 = 0.0, fi1 = 0.0, fi2 = 0.0;
-    unsigned flags = 0;
     uint32_t packed = 0xffffffffu;
     if (lane < mi) {
         const uint32_t e = __ldg(m.inc + e0 + lane);
         uint4 c = m.conn[e];
-        const bool active = !(c.x & 0x80000000u);
         c.x &= 0x7fffffffu;
         const uint32_t cn[4] = {c.x, c.y, c.z, c.w};
-        if (active) {
-            double x[12], ue[12];
+        const ElemRec<KT>& r = rec[e];
+        if (r.active != KT(0)) {
+            const int il = (cn[0] == n) ? 0 : (cn[1] == n) ? 1 : (cn[2] == n) ? 2 : 3;
+            fi0 = r.f[3 * il];
+            fi1 = r.f[3 * il + 1];
+            fi2 = r.f[3 * il + 2];
+            if (K != nullptr) {
 #pragma unroll
-            for (int a = 0; a < 4; ++a)
+                for (int q = 0; q < 12; ++q) S.d[lane][q] = r.d[q];
+                S.fI[lane][0] = (KT)fi0;
+                S.fI[lane][1] = (KT)fi1;
+                S.fI[lane][2] = (KT)fi2;
+                S.vabm[lane][0] = r.s[0];
+                S.vabm[lane][1] = r.s[1];
+                S.vabm[lane][2] = r.s[2];
+                packed = 0;
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    x[3 * a + d] = __ldg(m.xyz + 3 * (size_t)cn[a] + d);
-                    ue[3 * a + d] = __ldg(u + 3 * (size_t)cn[a] + d);
-                }
-            TetKin k;
-            if (tet_kinematics(x, ue, k)) {
-                double mu, lam;
-                material_of(m.mat_mode, m.m0, m.m1, e, m.mu_s, m.lam_s, m.c_mu, m.c_lam, mu,
-                            lam);
-                const Mandel M = mandel_stress(k.F, k.J, mu, lam);
-                const int il = (cn[0] == n) ? 0 : (cn[1] == n) ? 1 : (cn[2] == n) ? 2 : 3;
-                double dI[3];
-                grad_of(k, il, dI);
-                fi0 = k.vol * (M.m00 * dI[0] + M.m01 * dI[1] + M.m02 * dI[2]);
-                fi1 = k.vol * (M.m01 * dI[0] + M.m11 * dI[1] + M.m12 * dI[2]);
-                fi2 = k.vol * (M.m02 * dI[0] + M.m12 * dI[1] + M.m22 * dI[2]);
-                if (!(k.J > 0.0)) flags |= FM_FLAG_INVERTED;
-                if (k.J < kJSafe) flags |= FM_FLAG_J_CLAMPED;
-                if (!isfinite(fi0 + fi1 + fi2)) flags |= FM_FLAG_NONFINITE;
-                if (K != nullptr) {
-                    double a, b;
-                    tangent_ab(mu, lam, k.J, M.lnJ, m.inv_cnu, a, b);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) S.d[lane][3 * q + d] = (KT)k.d[q][d];
-                    S.fI[lane][0] = (KT)fi0;
-                    S.fI[lane][1] = (KT)fi1;
-                    S.fI[lane][2] = (KT)fi2;
-                    S.vabm[lane][0] = (KT)(k.vol * a);
-                    S.vabm[lane][1] = (KT)(k.vol * b);
-                    S.vabm[lane][2] = (KT)(k.vol * mu);
-                    packed = 0;
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int p = find_sorted(S.nbr, deg, cn[q]);
-                        packed |= (uint32_t)(p < 0 ? 0xff : p) << (8 * q);
-                        // edge lists as bitmasks: fixed bit order, deterministic
-                        if (p >= 0 && p != self_k) atomicOr(&S.members[p], 1u << lane);
-                    }
-                    if (!isfinite(a + b)) flags |= FM_FLAG_NONFINITE;
+                for (int q = 0; q < 4; ++q) {
+                    const int p = find_sorted(S.nbr, deg, cn[q]);
+                    packed |= (uint32_t)(p < 0 ? 0xff : p) << (8 * q);
+                    // edge lists as bitmasks: fixed bit order, deterministic
+                    if (p >= 0 && p != self_k) atomicOr(&S.members[p], 1u << lane);
                 }
             }
         }
@@ -142,7 +213,6 @@ __global__ void __launch_bounds__(kAsmWarps * 32, 3)
     S.f64[0][lane] = fi0;
     S.f64[1][lane] = fi1;
     S.f64[2][lane] = fi2;
-    if (flags) raise_flag(status, flags);
     __syncwarp();
 
     // internal force of the node: lane p < 3 sums component p over the
@@ -213,8 +283,14 @@ template <typename KT>
 static void launch_assemble_t(const MeshDev& m, const double* u, KT* K, double* f, double* R,
                               int apply_bc, unsigned* status, cudaStream_t s) {
     if (m.n_nodes == 0) return;
+    ElemRec<KT>* rec = static_cast<ElemRec<KT>*>(m.elem_rec);
+    if (m.n_elems) {
+        unsigned ge = (m.n_elems + 127) / 128;
+        if (ge > 148u * 32u) ge = 148u * 32u;
+        k_asm_elements<KT><<<ge, 128, 0, s>>>(m, u, rec, K != nullptr, status);
+    }
     const unsigned grid = (m.n_nodes + kAsmWarps - 1) / kAsmWarps;
-    k_assemble<KT><<<grid, kAsmWarps * 32, 0, s>>>(m, u, K, f, R, apply_bc, status);
+    k_assemble<KT><<<grid, kAsmWarps * 32, 0, s>>>(m, rec, K, f, R, apply_bc, status);
 }
 void launch_assemble(const MeshDev& m, const double* u, double* K, double* f, double* R,
                      int apply_bc, unsigned* status, cudaStream_t s) {

@@ -24,11 +24,17 @@ struct MeshDev {
     const double* m0 = nullptr;
     const double* m1 = nullptr;
     double mu_s = 0, lam_s = 0, c_mu = 0, c_lam = 0, inv_cnu = 0;
+    // per-element records of the assembly's element pass (n_elems *
+    // kElemRecBytes bytes, 16-byte aligned)
+    void* elem_rec = nullptr;
 };
+constexpr size_t kElemRecBytes = 224;
 
-// A10/A11/A12: node-owner assembly.  K (double or float, may be null for a
-// residual-only call), f (FP64, may be null), R = -f with zeros on
-// constrained DOFs (may be null).
+// A10/A11/A12: assembly in two passes, an element pass (each tet's
+// kinematics, stress, vertex forces and tangent scalars, once) and a
+// node-owner pass that writes every CSR row block once.  K (double or float,
+// may be null for a residual-only call), f (FP64, may be null), R = -f with
+// zeros on constrained DOFs (may be null).  m.elem_rec is required.
 void launch_assemble(const MeshDev& m, const double* u, double* K, double* f, double* R,
                      int apply_bc, unsigned* status, cudaStream_t s);
 void launch_assemble(const MeshDev& m, const double* u, float* K, double* f, double* R,

@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="flexmesh", choices=["flexmesh", "reference"])
     ap.add_argument("--N", type=int, default=64)
-    ap.add_argument("--inner-tol", type=float, default=0.1)
+    ap.add_argument("--inner-tol", type=float, default=0.2)
     ap.add_argument("--fp64-steps", type=int, default=1,
                     help="timed FP64 load steps for the mixed/FP64 comparison (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
