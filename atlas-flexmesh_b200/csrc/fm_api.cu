@@ -111,6 +111,7 @@ struct fm_ctx {
     DevBuf<unsigned char> cl_pack32_f, cl_pack32_b, cl_pack64_f, cl_pack64_b;
     fm::ClusterSolve cl_f, cl_b;
     bool cl_ok32 = false, cl_ok64 = false;
+    bool cl_lanes = false;  // one lane per node (fm_trsv_lanes.cu); cl_card_* = group starts
     std::vector<uint32_t> lvl_fwd_ptr, lvl_fwd_rows, lvl_bwd_ptr, lvl_bwd_rows;
 
     // material
@@ -381,6 +382,87 @@ fm::NodeSched node_sched(const fm_ctx* c) {
     return S;
 }
 
+// Plans for the one-lane-per-node cluster solves (fm_trsv_lanes.cu): a
+// 16-CTA cluster of 6 warps each; every level's groups of 32 nodes must fit
+// the cluster's warps once, and the neighbours per side the lane limit.
+fm_status setup_lane_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
+                            const std::vector<uint32_t>& lo, const std::vector<uint32_t>& up,
+                            const std::vector<uint32_t>& uo) {
+    constexpr uint32_t kCs = 16, kWarps = 6, kMaxSlots = 4096;
+    constexpr size_t kMaxSmem = 227 * 1024;
+    const char* wenv = getenv("FM_TRSV_WINDOW");
+    const uint32_t window = wenv ? std::max(1u, (uint32_t)strtoul(wenv, nullptr, 10)) : 8u;
+    fm::ClusterPlan pf, pb;
+    std::vector<uint32_t> nslot;
+    if (!fm::cluster_plan(c->graph, true, lp, lo, kCs, kWarps, window, kMaxSlots, pf, nslot, true) ||
+        !fm::cluster_plan(c->graph, false, up, uo, kCs, kWarps, window, kMaxSlots, pb, nslot, true))
+        return FM_OK;
+    if (pf.max_per_warp > 1 || pb.max_per_warp > 1) return FM_OK;
+    if (pf.max_cnt > (uint32_t)fm::lanes_max_neighbours() ||
+        pb.max_cnt > (uint32_t)fm::lanes_max_neighbours())
+        return FM_OK;
+    auto view = [](const fm::ClusterPlan& p) {
+        fm::ClusterSolve v;
+        v.n_levels = p.n_levels;
+        v.n_ctas = p.n_ctas;
+        v.warps_per_cta = p.warps_per_cta;
+        v.max_per_warp = 1;
+        v.maxc = std::max(p.max_cnt, 1u);
+        v.pool_slots = std::max(p.slots_per_cta, 1u);
+        v.window = p.window;
+        v.n_groups = p.n_groups;
+        const char* sl = getenv("FM_TRSV_SLEEP_NS");
+        v.sleep_ns = sl ? (uint32_t)strtoul(sl, nullptr, 10) : 0u;
+        return v;
+    };
+    fm::ClusterSolve f = view(pf), b = view(pb);
+    auto fits = [&](size_t vb) {
+        const size_t sm = std::max(fm::lanes_smem_bytes(f, vb), fm::lanes_smem_bytes(b, vb));
+        return sm <= kMaxSmem && fm::lanes_max_active(vb, f) >= 1 && fm::lanes_max_active(vb, b) >= 1;
+    };
+    const bool ok32 = fits(4), ok64 = fits(8);
+    if (!ok32 && !ok64) return FM_OK;
+    auto group_first = [](const fm::ClusterPlan& p) {
+        std::vector<uint32_t> gf(p.n_groups + 1, 0);
+        for (uint32_t l = 0; l < p.n_levels; ++l)
+            for (uint32_t g = p.lvl_gptr[l]; g < p.lvl_gptr[l + 1]; ++g)
+                gf[g] = p.lvl_ptr[l] + 32 * (g - p.lvl_gptr[l]);
+        gf[p.n_groups] = p.n_levels ? p.lvl_ptr[p.n_levels] : 0;
+        return gf;
+    };
+    const std::vector<uint32_t> gff = group_first(pf), gfb = group_first(pb);
+    CK(upload(c->cl_lvl_f, pf.lvl_gptr.data(), pf.lvl_gptr.size(), c->stream));
+    CK(upload(c->cl_lvl_b, pb.lvl_gptr.data(), pb.lvl_gptr.size(), c->stream));
+    CK(upload(c->cl_rec_f, reinterpret_cast<const uint4*>(pf.rec.data()), pf.rec.size() / 4,
+              c->stream));
+    CK(upload(c->cl_rec_b, reinterpret_cast<const uint4*>(pb.rec.data()), pb.rec.size() / 4,
+              c->stream));
+    CK(upload(c->cl_nslot, nslot.data(), nslot.size(), c->stream));
+    CK(upload(c->cl_rptr_f, pf.reset_ptr.data(), pf.reset_ptr.size(), c->stream));
+    CK(upload(c->cl_rptr_b, pb.reset_ptr.data(), pb.reset_ptr.size(), c->stream));
+    CK(upload(c->cl_reset_f, pf.reset.data(), pf.reset.size(), c->stream));
+    CK(upload(c->cl_reset_b, pb.reset.data(), pb.reset.size(), c->stream));
+    CK(upload(c->cl_card_f, gff.data(), gff.size(), c->stream));
+    CK(upload(c->cl_card_b, gfb.data(), gfb.size(), c->stream));
+    f.lvl_ptr = c->cl_lvl_f.p;
+    f.rec = c->cl_rec_f.p;
+    f.nslot = c->cl_nslot.p;
+    f.reset_ptr = c->cl_rptr_f.p;
+    f.reset = c->cl_reset_f.p;
+    b.lvl_ptr = c->cl_lvl_b.p;
+    b.rec = c->cl_rec_b.p;
+    b.nslot = c->cl_nslot.p;
+    b.reset_ptr = c->cl_rptr_b.p;
+    b.reset = c->cl_reset_b.p;
+    c->cl_f = f;
+    c->cl_b = b;
+    c->cl_ok32 = ok32;
+    c->cl_ok64 = ok64;
+    c->cl_lanes = true;
+    CK(cudaStreamSynchronize(c->stream));
+    return FM_OK;
+}
+
 // Plans for the cluster solves: the largest cluster (16, then 8 CTAs of 32
 // warps) whose plan fits and that the device can make resident.  Selected
 // with FM_TRSV_PATH=cluster in the environment; the grid-wide pipelined
@@ -389,8 +471,11 @@ fm_status setup_cluster_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
                                const std::vector<uint32_t>& lo, const std::vector<uint32_t>& up,
                                const std::vector<uint32_t>& uo) {
     c->cl_ok32 = c->cl_ok64 = false;
+    c->cl_lanes = false;
     const char* path = getenv("FM_TRSV_PATH");
-    if (!path || std::strcmp(path, "cluster") != 0) return FM_OK;
+    if (!path) return FM_OK;
+    if (std::strcmp(path, "lanes") == 0) return setup_lane_solves(c, lp, lo, up, uo);
+    if (std::strcmp(path, "cluster") != 0) return FM_OK;
     constexpr uint32_t kWarps = 32, kMaxSlots = 4096;
     constexpr size_t kMaxSmem = 227 * 1024;
     const char* wenv = getenv("FM_TRSV_WINDOW");
@@ -469,10 +554,15 @@ int precond_nodes(fm_ctx* c, const T* lu, const T* dinv, const T* r, T* tmp, T* 
                   unsigned* status) {
     const bool cl = sizeof(T) == 4 ? c->cl_ok32 : c->cl_ok64;
     if (cl && c->nn) {
-        if (fm::launch_trsv_cluster<T>(c->cl_f, c->cl_b, packed_cards<T>(c, true).p,
-                                       packed_cards<T>(c, false).p, r, tmp, z, status,
-                                       c->stream) == cudaSuccess)
-            return 2;
+        const cudaError_t e =
+            c->cl_lanes
+                ? fm::launch_trsv_lanes<T>(c->cl_f, c->cl_b, c->cl_card_f.p, c->cl_card_b.p,
+                                           packed_cards<T>(c, true).p, packed_cards<T>(c, false).p,
+                                           r, tmp, z, status, c->stream)
+                : fm::launch_trsv_cluster<T>(c->cl_f, c->cl_b, packed_cards<T>(c, true).p,
+                                             packed_cards<T>(c, false).p, r, tmp, z, status,
+                                             c->stream);
+        if (e == cudaSuccess) return 2;
         // a launch the device refuses: the pipelined solves from now on
         cudaGetLastError();
         c->cl_ok32 = c->cl_ok64 = false;
@@ -578,10 +668,17 @@ fm_status ilu_core(fm_ctx* c, SolverCsr& S, const T* a, T* lu, T* diag) {
             // the cluster solves read the factors as packed cards
             DevBuf<unsigned char>& pf = packed_cards<T>(c, true);
             DevBuf<unsigned char>& pb = packed_cards<T>(c, false);
-            CK(pf.reserve((size_t)c->nn * fm::cluster_card_bytes(c->cl_f, sizeof(T))));
-            CK(pb.reserve((size_t)c->nn * fm::cluster_card_bytes(c->cl_b, sizeof(T))));
-            fm::launch_pack_cards<T>(c->cl_f, c->cl_b, c->cl_card_f.p, c->cl_card_b.p, c->nn, lu,
-                                     work<T>(c).dinv.p, pf.p, pb.p, c->stream);
+            if (c->cl_lanes) {
+                CK(pf.reserve((size_t)c->cl_f.n_groups * fm::lanes_card_bytes(c->cl_f, sizeof(T))));
+                CK(pb.reserve((size_t)c->cl_b.n_groups * fm::lanes_card_bytes(c->cl_b, sizeof(T))));
+                fm::launch_pack_groups<T>(c->cl_f, c->cl_b, c->cl_card_f.p, c->cl_card_b.p, lu,
+                                          work<T>(c).dinv.p, pf.p, pb.p, c->stream);
+            } else {
+                CK(pf.reserve((size_t)c->nn * fm::cluster_card_bytes(c->cl_f, sizeof(T))));
+                CK(pb.reserve((size_t)c->nn * fm::cluster_card_bytes(c->cl_b, sizeof(T))));
+                fm::launch_pack_cards<T>(c->cl_f, c->cl_b, c->cl_card_f.p, c->cl_card_b.p, c->nn,
+                                         lu, work<T>(c).dinv.p, pf.p, pb.p, c->stream);
+            }
             CK(cudaGetLastError());
         }
         return FM_OK;

@@ -162,7 +162,7 @@ uint32_t csr_levels(uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx
 bool cluster_plan(const NodeGraph& g, bool lower, const std::vector<uint32_t>& ptr,
                   const std::vector<uint32_t>& order, uint32_t n_ctas, uint32_t warps_per_cta,
                   uint32_t window, uint32_t max_slots_per_cta, ClusterPlan& plan,
-                  std::vector<uint32_t>& nslot) {
+                  std::vector<uint32_t>& nslot, bool lanes) {
     const uint32_t n = g.n_nodes;
     const uint32_t nl = ptr.empty() ? 0 : (uint32_t)ptr.size() - 1;
     const uint32_t W = n_ctas * warps_per_cta;
@@ -175,11 +175,22 @@ bool cluster_plan(const NodeGraph& g, bool lower, const std::vector<uint32_t>& p
     plan.window = window;
     plan.lvl_ptr = ptr;
     plan.rec.assign(4 * (size_t)n, 0);
+    plan.lanes = lanes;
+    plan.lvl_gptr.assign(nl + 1, 0);
+    for (uint32_t l = 0; l < nl; ++l)
+        plan.lvl_gptr[l + 1] = plan.lvl_gptr[l] + (ptr[l + 1] - ptr[l] + 31) / 32;
+    plan.n_groups = plan.lvl_gptr[nl];
+    // warp of position p of level l
+    auto warp_of = [&](uint32_t l, uint32_t p) {
+        const uint32_t i = p - ptr[l];
+        return lanes ? (plan.lvl_gptr[l] + i / 32) % W : i % W;
+    };
     nslot.resize(g.nbr.size(), 0);
     std::vector<uint32_t> level(n), pos(n), last(n);
     for (uint32_t l = 0; l < nl; ++l) {
         const uint32_t width = ptr[l + 1] - ptr[l];
-        plan.max_per_warp = std::max(plan.max_per_warp, (width + W - 1) / W);
+        const uint32_t units = lanes ? (width + 31) / 32 : width;
+        plan.max_per_warp = std::max(plan.max_per_warp, (units + W - 1) / W);
         for (uint32_t p = ptr[l]; p < ptr[l + 1]; ++p) {
             level[order[p]] = l;
             pos[order[p]] = p;
@@ -212,7 +223,7 @@ bool cluster_plan(const NodeGraph& g, bool lower, const std::vector<uint32_t>& p
             release[l / window].clear();
         }
         for (uint32_t p = ptr[l]; p < ptr[l + 1]; ++p) {
-            const uint32_t gw = (p - ptr[l]) % W;
+            const uint32_t gw = warp_of(l, p);
             const uint32_t cta = gw / warps_per_cta;
             uint32_t idx;
             if (!free_list[cta].empty()) {

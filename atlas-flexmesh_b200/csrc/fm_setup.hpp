@@ -81,6 +81,12 @@ struct ClusterPlan {
     // slots CTA c resets after window t: reset[reset_ptr[t * n_ctas + c] ...
     // reset_ptr[t * n_ctas + c + 1])
     std::vector<uint32_t> reset_ptr, reset;
+    // lane groups (lanes = true): a level's positions in groups of 32, group
+    // i of level l is global group lvl_gptr[l] + i, taken by warp
+    // (global group) mod W, lane = position within the group
+    bool lanes = false;
+    uint32_t n_groups = 0;
+    std::vector<uint32_t> lvl_gptr;  // n_levels + 1
 };
 
 // Builds the plan of one direction (lower: forward solve over the levels
@@ -93,7 +99,7 @@ struct ClusterPlan {
 bool cluster_plan(const NodeGraph& g, bool lower, const std::vector<uint32_t>& ptr,
                   const std::vector<uint32_t>& order, uint32_t n_ctas, uint32_t warps_per_cta,
                   uint32_t window, uint32_t max_slots_per_cta, ClusterPlan& plan,
-                  std::vector<uint32_t>& nslot);
+                  std::vector<uint32_t>& nslot, bool lanes = false);
 
 // Structural map of the ILU(0) updates (node granularity): for node n and
 // its k-th lower neighbour m (k < self[n]), entry t of

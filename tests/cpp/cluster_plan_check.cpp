@@ -46,12 +46,14 @@ int main(int argc, char** argv) {
     for (int lower = 1; lower >= 0; --lower) {
         std::vector<uint32_t> ptr, order;
         node_levels(g, lower != 0, ptr, order);
+        for (int lanes = 0; lanes < 2; ++lanes)
         for (uint32_t cs : {8u, 16u})
         for (uint32_t win : {1u, 8u}) {
-            const uint32_t wpc = 32, W = cs * wpc;
+            const uint32_t wpc = lanes ? 6 : 32, W = cs * wpc;
             ClusterPlan P;
             std::vector<uint32_t> nslot;
-            if (!cluster_plan(g, lower != 0, ptr, order, cs, wpc, win, 1u << 16, P, nslot))
+            if (!cluster_plan(g, lower != 0, ptr, order, cs, wpc, win, 1u << 16, P, nslot,
+                              lanes != 0))
                 return fail("plan refused", cs, lower);
             std::vector<long> level(nn, -1), slot(nn, -1), last(nn, -1);
             for (uint32_t l = 0; l < P.n_levels; ++l)
@@ -64,7 +66,9 @@ int main(int argc, char** argv) {
                     if (r[1] != g.ptr[n] || deg != g.ptr[n + 1] - g.ptr[n] || sk != g.self[n] ||
                         cnt != (lower ? sk : deg - sk - 1))
                         return fail("record", p, n);
-                    const uint32_t cta = ((p - P.lvl_ptr[l]) % W) / wpc;
+                    const uint32_t i = p - P.lvl_ptr[l];
+                    const uint32_t warp = lanes ? (P.lvl_gptr[l] + i / 32) % W : i % W;
+                    const uint32_t cta = warp / wpc;
                     if (r[3] >= P.slots_per_cta) return fail("slot range", p, r[3]);
                     slot[n] = (long)((cta << 16) | r[3]);
                 }
@@ -106,6 +110,17 @@ int main(int argc, char** argv) {
                         ++listed;
                     }
             if (listed != (long)nn) return fail("reset count", listed, nn);
+            if (lanes) {
+                // lane groups: ceil(width / 32) per level, numbered consecutively
+                uint32_t gsum = 0;
+                for (uint32_t l = 0; l < P.n_levels; ++l) {
+                    if (P.lvl_gptr[l] != gsum) return fail("group ptr", l, gsum);
+                    gsum += (P.lvl_ptr[l + 1] - P.lvl_ptr[l] + 31) / 32;
+                }
+                if (P.lvl_gptr[P.n_levels] != gsum || P.n_groups != gsum)
+                    return fail("group count", gsum, P.n_groups);
+                continue;
+            }
             // cards: a bijection onto [0, nn) that keeps each level's cards in
             // the level's range and each warp's cards of a level consecutive
             std::vector<uint32_t> card;
