@@ -10,7 +10,8 @@
 //   * a slot is handed out again only from the second window after the
 //     window of its last read, and each retirement is listed once in the
 //     reset list of that window and the slot's CTA;
-//   * slots stay inside their CTA's pool and belong to the writer's CTA.
+//   * slots stay inside their CTA's pool and belong to the writer's CTA;
+// and the ILU(0) update map (ilu_edge_maps) against a direct search.
 // Prints "ok" and exits 0, or names the first violation and exits 1.
 #include <algorithm>
 #include <cstdio>
@@ -134,6 +135,27 @@ int main(int argc, char** argv) {
                     const uint32_t i = p - P.lvl_ptr[l];
                     if (i >= W && card[p - W] + 1 != c) return fail("card order", p, c);
                 }
+        }
+    }
+    // ILU(0) update map: for node i and lower neighbour m, entry t names the
+    // position in i's list of m's neighbour self(m) + t, or 0xff
+    {
+        std::vector<uint32_t> eptr;
+        std::vector<uint8_t> emap;
+        ilu_edge_maps(g, eptr, emap);
+        if (eptr.size() != nn + 1 || emap.size() != eptr[nn]) return fail("edge map size", 0, 0);
+        for (uint32_t i = 0; i < nn; ++i) {
+            uint32_t o = eptr[i];
+            for (uint32_t k = g.ptr[i]; k < g.ptr[i] + g.self[i]; ++k) {
+                const uint32_t m = g.nbr[k];
+                for (uint32_t q = g.ptr[m] + g.self[m]; q < g.ptr[m + 1]; ++q, ++o) {
+                    uint32_t want = 0xff;
+                    for (uint32_t r = g.ptr[i]; r < g.ptr[i + 1]; ++r)
+                        if (g.nbr[r] == g.nbr[q]) want = r - g.ptr[i];
+                    if (emap[o] != want) return fail("edge map entry", i, o);
+                }
+            }
+            if (o != eptr[i + 1]) return fail("edge map extent", i, o);
         }
     }
     std::printf("ok\n");
