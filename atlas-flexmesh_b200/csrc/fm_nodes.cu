@@ -120,7 +120,7 @@ __device__ __forceinline__ void ilu_step(IluStage<T>& G, T (&w)[3][3], int k, in
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kNodeWarps * 32)
+__global__ void __launch_bounds__(kNodeWarps * 32, sizeof(T) == 4 ? 3 : 2)
     k_ilu0_nodes(NodeSched S, const T* __restrict__ a, T* __restrict__ lu, T* __restrict__ dg,
                  T* __restrict__ dinv, unsigned* __restrict__ done, unsigned epoch,
                  unsigned* __restrict__ status, unsigned sleep_ns) {
@@ -162,12 +162,51 @@ __global__ void __launch_bounds__(kNodeWarps * 32)
             if (lane >= o) incl += v;
         }
         const uint32_t eb = __ldg(S.emap_ptr + n);
+        const uint32_t tot = __shfl_sync(kFull, incl, 31);  // pairs of all lower neighbours
         __syncwarp();  // the previous node's reads of G are done
         G.poff[lane] = incl - np;
         if (lane == 31) G.poff[32] = incl;
         G.mb0[lane] = mb0;
         G.mdeg[lane] = (uint8_t)mdeg;
         G.msk[lane] = (uint8_t)msk;
+        // staged rows are padded to whole 32-column slots (zeros beyond rl), so
+        // the updates need no column mask
+        const int nsl = (rl + 31) >> 5;
+        const int rs = 32 * nsl;
+        const int cap_k = UCAP / (3 * rs) > 0 ? UCAP / (3 * rs) : 1;
+        // Usual case (all lower neighbours in one stage, one round of pairs per
+        // lane): everything structural about the staging — the zeroed stage,
+        // each pair's neighbour, source row and destination column — is done
+        // before the wait, so after it only the U values are loaded.
+        const bool fast = sk > 0 && sk <= cap_k && sk <= kStageNbrs &&
+                          tot <= (uint32_t)(32 * kPairRound);
+        const T* fsrc[kPairRound];
+        int fmrl[kPairRound], fjb[kPairRound], flim[kPairRound], fdst[kPairRound];
+        uint32_t fpos[kPairRound];
+        if (fast) {
+            for (int i = lane; i < sk * 3 * rs; i += 32) G.u[i] = T(0);
+            __syncwarp();
+#pragma unroll
+            for (int r = 0; r < kPairRound; ++r) {
+                const uint32_t pr = lane + 32 * r;
+                fpos[r] = 0xffu;
+                fdst[r] = 0;
+                fsrc[r] = nullptr;
+                fmrl[r] = fjb[r] = flim[r] = 0;
+                if (pr < tot) {
+                    int k = 0;
+                    for (int kk = 1; kk < sk; ++kk) k += (int)(G.poff[kk] <= pr);
+                    fpos[r] = __ldg(S.emap + eb + pr);
+                    const int ms = G.msk[k];
+                    const int kk = ms + (int)(pr - G.poff[k]);
+                    fmrl[r] = 3 * (int)G.mdeg[k];
+                    fjb[r] = 3 * kk;
+                    flim[r] = 3 * ms;
+                    fsrc[r] = lu + 9 * (size_t)G.mb0[k] + 3 * kk;
+                    fdst[r] = (k * 3) * rs;
+                }
+            }
+        }
         // wait for every lower neighbour node's rows
         const bool ok = wait_flags_warp(done + (lane < sk ? my_nbr : 0), lane < sk, epoch,
                                         status, sleep_ns);
@@ -178,12 +217,34 @@ __global__ void __launch_bounds__(kNodeWarps * 32)
             dv2 = ld_cg(dinv + 3 * (size_t)my_nbr + 2);
         }
         __syncwarp();
-        // staged rows are padded to whole 32-column slots (zeros beyond rl), so
-        // the updates need no column mask
-        const int nsl = (rl + 31) >> 5;
-        const int rs = 32 * nsl;
-        const int cap_k = UCAP / (3 * rs) > 0 ? UCAP / (3 * rs) : 1;
-        for (int k0 = 0; ok && k0 < sk; k0 += cap_k) {
+        if (ok && fast) {
+            T val[kPairRound][9];
+#pragma unroll
+            for (int r = 0; r < kPairRound; ++r)
+                if (fpos[r] != 0xffu)
+#pragma unroll
+                    for (int q = 0; q < 3; ++q)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+                            val[r][3 * q + c] = fjb[r] + c > flim[r] + q
+                                                    ? ld_cg(fsrc[r] + (size_t)q * fmrl[r] + c)
+                                                    : T(0);
+#pragma unroll
+            for (int r = 0; r < kPairRound; ++r)
+                if (fpos[r] != 0xffu) {
+                    const int d = fdst[r] + 3 * (int)fpos[r];
+#pragma unroll
+                    for (int q = 0; q < 3; ++q)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) G.u[d + q * rs + c] = val[r][3 * q + c];
+                }
+            __syncwarp();
+#pragma unroll
+            for (int k = 0; k < kStageNbrs; ++k)
+                if (k < sk) ilu_step(G, w, k, 0, rs, nsl, lane, dv0, dv1, dv2);
+            __syncwarp();
+        }
+        for (int k0 = 0; ok && !fast && k0 < sk; k0 += cap_k) {
             const int k1 = k0 + cap_k < sk ? k0 + cap_k : sk;
             const int nu = (k1 - k0) * 3 * rs;
             for (int i = lane; i < nu; i += 32) G.u[i] = T(0);
