@@ -129,6 +129,7 @@ struct fm_ctx {
     DevBuf<int32_t> ref_slot;
     DevBuf<double> ke_scratch;
     DevBuf<unsigned char> elem_rec;  // assembly element-pass records
+    DevBuf<uint32_t> inc_pos, nbr_members;  // node-pass scatter structure
 
     // solver state
     Work<double> w64;
@@ -291,6 +292,8 @@ fm::MeshDev mesh_view(const fm_ctx* c) {
     m.c_lam = c->c_lam;
     m.inv_cnu = c->inv_cnu;
     m.elem_rec = c->elem_rec.p;
+    m.inc_pos = c->inc_pos.p;
+    m.nbr_members = c->nbr_members.p;
     return m;
 }
 
@@ -901,6 +904,32 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
         CK(c->vec_a.reserve(c->n));
         CK(c->vec_b.reserve(c->n));
         CK(c->elem_rec.reserve(std::max<size_t>(1, (size_t)c->ne * fm::kElemRecBytes)));
+        {
+            // node-pass scatter structure: for every (node, incident tet) the
+            // tet's vertex positions in the node's neighbour list, and for
+            // every (node, neighbour) the incident tets on that edge
+            std::vector<uint32_t> ipos(c->inc.elem.size(), 0xffffffffu);
+            std::vector<uint32_t> memb(c->graph.nbr.size(), 0u);
+            for (uint32_t nd = 0; nd < c->nn; ++nd) {
+                const uint32_t* nl = c->graph.nbr.data() + c->graph.ptr[nd];
+                const uint32_t deg = c->graph.ptr[nd + 1] - c->graph.ptr[nd];
+                for (uint32_t i = c->inc.ptr[nd]; i < c->inc.ptr[nd + 1]; ++i) {
+                    const uint32_t e = c->inc.elem[i], l = i - c->inc.ptr[nd];
+                    uint32_t pk = 0;
+                    for (int q = 0; q < 4; ++q) {
+                        const uint32_t v = conn[4 * (size_t)e + q];
+                        const uint32_t* hit = std::lower_bound(nl, nl + deg, v);
+                        const uint32_t p = (hit != nl + deg && *hit == v) ? (uint32_t)(hit - nl) : 0xffu;
+                        pk |= p << (8 * q);
+                        if (p != 0xffu && v != nd && !c->h_skip[e])
+                            memb[c->graph.ptr[nd] + p] |= 1u << l;
+                    }
+                    ipos[i] = pk;
+                }
+            }
+            CK(upload(c->inc_pos, ipos.data(), ipos.size(), c->stream));
+            CK(upload(c->nbr_members, memb.data(), memb.size(), c->stream));
+        }
         CK(cudaStreamSynchronize(c->stream));
     } catch (const std::bad_alloc&) {
         return fail(c, FM_ERR_OOM, "host allocation failed in fm_set_mesh");

@@ -32,8 +32,6 @@ struct AsmStage {
     KT vabm[32][3];   // vol*a, vol*b, vol*mu (tangent scalars)
     double f64[3][32];  // FP64 node-force contributions of the incident tets
     uint32_t pos[32]; // 4 x u8: position of each tet node in the owner's neighbour list
-    uint32_t nbr[32];
-    uint32_t members[32];  // bit l of members[k]: tet l holds the edge (owner, nbr[k])
 };
 
 __device__ __forceinline__ int find_sorted(const uint32_t* a, int len, uint32_t key) {
@@ -171,42 +169,34 @@ __global__ void __launch_bounds__(kAsmWarps * 32, 3)
     const uint32_t e0 = m.inc_ptr[n];
     const int mi = (int)(m.inc_ptr[n + 1] - e0);
     const uint32_t my_nbr = lane < deg ? __ldg(m.nbr + nb0 + lane) : 0xffffffffu;
-    S.nbr[lane] = my_nbr;
-    S.members[lane] = 0u;
     const int self_k = __ffs(__ballot_sync(kFull, my_nbr == n)) - 1;
-    __syncwarp();
+    // edge lists of the tangent blocks: structural, built on the host
+    const uint32_t my_members = (K != nullptr && lane < deg) ? __ldg(m.nbr_members + nb0 + lane) : 0u;
 
     double fi0 = 0.0, fi1 = 0.0, fi2 = 0.0;
     uint32_t packed = 0xffffffffu;
     if (lane < mi) {
         const uint32_t e = __ldg(m.inc + e0 + lane);
-        uint4 c = m.conn[e];
-        c.x &= 0x7fffffffu;
-        const uint32_t cn[4] = {c.x, c.y, c.z, c.w};
+        packed = __ldg(m.inc_pos + e0 + lane);
         const ElemRec<KT>& r = rec[e];
-        if (r.active != KT(0)) {
-            const int il = (cn[0] == n) ? 0 : (cn[1] == n) ? 1 : (cn[2] == n) ? 2 : 3;
+        const bool act = r.active != KT(0);
+        if (act) {
+            const int il = byte_index(packed, (uint32_t)self_k);
             fi0 = r.f[3 * il];
             fi1 = r.f[3 * il + 1];
             fi2 = r.f[3 * il + 2];
-            if (K != nullptr) {
+        }
+        if (K != nullptr) {
+            // an inactive tet (degenerate at this state) stays in the edge
+            // lists with zero data: it adds exact zeros
 #pragma unroll
-                for (int q = 0; q < 12; ++q) S.d[lane][q] = r.d[q];
-                S.fI[lane][0] = (KT)fi0;
-                S.fI[lane][1] = (KT)fi1;
-                S.fI[lane][2] = (KT)fi2;
-                S.vabm[lane][0] = r.s[0];
-                S.vabm[lane][1] = r.s[1];
-                S.vabm[lane][2] = r.s[2];
-                packed = 0;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int p = find_sorted(S.nbr, deg, cn[q]);
-                    packed |= (uint32_t)(p < 0 ? 0xff : p) << (8 * q);
-                    // edge lists as bitmasks: fixed bit order, deterministic
-                    if (p >= 0 && p != self_k) atomicOr(&S.members[p], 1u << lane);
-                }
-            }
+            for (int q = 0; q < 12; ++q) S.d[lane][q] = act ? r.d[q] : KT(0);
+            S.fI[lane][0] = (KT)fi0;
+            S.fI[lane][1] = (KT)fi1;
+            S.fI[lane][2] = (KT)fi2;
+            S.vabm[lane][0] = act ? r.s[0] : KT(0);
+            S.vabm[lane][1] = act ? r.s[1] : KT(0);
+            S.vabm[lane][2] = act ? r.s[2] : KT(0);
         }
     }
     S.pos[lane] = packed;
@@ -233,7 +223,7 @@ __global__ void __launch_bounds__(kAsmWarps * 32, 3)
 #pragma unroll
     for (int q = 0; q < 9; ++q) acc[q] = KT(0);
     if (lane < deg && lane != self_k) {
-        uint32_t members = S.members[lane];
+        uint32_t members = my_members;
         while (members) {
             const int l = __ffs(members) - 1;
             members &= members - 1;

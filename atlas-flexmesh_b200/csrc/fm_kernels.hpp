@@ -27,6 +27,12 @@ struct MeshDev {
     // per-element records of the assembly's element pass (n_elems *
     // kElemRecBytes bytes, 16-byte aligned)
     void* elem_rec = nullptr;
+    // structural scatter data of the node pass, built once per mesh:
+    // inc_pos[i]: positions (4 x u8) of incidence i's tet vertices in the
+    // owner's neighbour list; nbr_members[j]: bit l set when the owner's
+    // l-th incident tet (not skipped) holds the edge to neighbour entry j
+    const uint32_t* inc_pos = nullptr;
+    const uint32_t* nbr_members = nullptr;
 };
 constexpr size_t kElemRecBytes = 224;
 
