@@ -67,12 +67,6 @@ template <typename T>
 __device__ __forceinline__ T pick3(const T v[3], int s) {
     return s == 0 ? v[0] : s == 1 ? v[1] : v[2];
 }
-template <typename T>
-__device__ __forceinline__ void put3(T v[3], int s, T x) {
-    if (s == 0) v[0] = x;
-    else if (s == 1) v[1] = x;
-    else v[2] = x;
-}
 
 // Elimination against lower neighbour k (the node's columns 3k .. 3k+2):
 // multipliers by forward substitution through the neighbour's own U block,

@@ -45,60 +45,10 @@ __device__ __forceinline__ void st_relaxed(float* p, float v) {
     asm volatile("st.relaxed.gpu.global.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
 }
 
-// Spin (bounded) until *p is not the sentinel; returns the value, or the
-// sentinel when the wait gave up (FM_FLAG_TIMEOUT then set).
-// backoff_ns > 0: sleep between polls, doubling from backoff_ns up to 8x,
-// which keeps thousands of early waiters from flooding L2 with polls.
-template <typename T>
-__device__ __forceinline__ T wait_value(const T* p, unsigned* status, unsigned backoff_ns = 0) {
-    T v = ld_relaxed(p);
-    if (!Sentinel<T>::is(v)) return v;
-    const long long t0 = clock64();
-    unsigned ns = backoff_ns;
-    for (unsigned it = 1;; ++it) {
-        if (ns) {
-            __nanosleep(ns);
-            if (ns < 8 * backoff_ns) ns <<= 1;
-        }
-        v = ld_relaxed(p);
-        if (!Sentinel<T>::is(v)) return v;
-        if ((it & 63u) == 0) {
-            if (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) return v;
-            if (clock64() - t0 > kWaitCycles) {
-                raise_flag(status, FM_FLAG_TIMEOUT);
-                return v;
-            }
-        }
-    }
-}
-
-// Three consecutive values (one node's block) with the polls in flight
-// together: one round trip when they are ready, not three.
-template <typename T>
-__device__ __forceinline__ void wait_values3(const T* p, unsigned* status, T& v0, T& v1, T& v2) {
-    v0 = ld_relaxed(p);
-    v1 = ld_relaxed(p + 1);
-    v2 = ld_relaxed(p + 2);
-    if (!(Sentinel<T>::is(v0) | Sentinel<T>::is(v1) | Sentinel<T>::is(v2))) return;
-    const long long t0 = clock64();
-    for (unsigned it = 1;; ++it) {
-        if (Sentinel<T>::is(v0)) v0 = ld_relaxed(p);
-        if (Sentinel<T>::is(v1)) v1 = ld_relaxed(p + 1);
-        if (Sentinel<T>::is(v2)) v2 = ld_relaxed(p + 2);
-        if (!(Sentinel<T>::is(v0) | Sentinel<T>::is(v1) | Sentinel<T>::is(v2))) return;
-        if ((it & 63u) == 0) {
-            if (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) return;
-            if (clock64() - t0 > kWaitCycles) {
-                raise_flag(status, FM_FLAG_TIMEOUT);
-                return;
-            }
-        }
-    }
-}
-
-// Warp-uniform form of wait_values3: lanes with p != nullptr wait for their
-// node's three values, and all lanes leave together (warp vote), so the
-// warp stays converged for the reduction that follows.  After 16 polls the
+// Bounded wait for a node's three values: lanes with p != nullptr wait for
+// them, and all lanes leave together (warp vote), so the warp stays
+// converged for the reduction that follows.  On a timeout FM_FLAG_TIMEOUT
+// is set and the values may still be sentinels.  After 16 polls the
 // loop sleeps between polls, doubling from 32 ns up to sleep_ns (0: never).
 template <typename T>
 __device__ __forceinline__ void wait_values3_warp(const T* p, unsigned* status, unsigned sleep_ns,
