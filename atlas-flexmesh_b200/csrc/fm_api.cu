@@ -113,6 +113,12 @@ struct fm_ctx {
     bool cl_ok32 = false, cl_ok64 = false;
     bool cl_lanes = false;  // one lane per node (fm_trsv_lanes.cu); cl_card_* = group starts
     std::vector<uint32_t> lvl_fwd_ptr, lvl_fwd_rows, lvl_bwd_ptr, lvl_bwd_rows;
+    // slab-partitioned push solves (fm_trsv_push.cu): plan on the device and
+    // whether they run in FP32 / FP64
+    DevBuf<uint32_t> pu_pos_f, pu_pos_b, pu_src, pu_push_f, pu_push_b, pu_nslot_f, pu_nslot_b;
+    DevBuf<uint4> pu_rec_f, pu_rec_b;
+    fm::PushSolve pu;
+    bool pu_ok32 = false, pu_ok64 = false;
 
     // material
     bool has_mat = false;
@@ -385,6 +391,84 @@ fm::NodeSched node_sched(const fm_ctx* c) {
     return S;
 }
 
+// Plan of the slab-partitioned push solves (fm_trsv_push.cu): one slab per
+// cluster of 8 CTAs, as many clusters as the device keeps resident (FP32 and
+// FP64 kernels alike), when every CTA's slots fit its shared memory (the
+// plan first tries to fit FP64 slots, else FP32 only).  Selected with
+// FM_TRSV_PATH=push; FM_TRSV_PUSH_WARPS sets the warps per CTA (default 16),
+// FM_TRSV_PUSH_BLOCK the interleave block (default: chosen by the plan).
+fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
+                            const std::vector<uint32_t>& lo, const std::vector<uint32_t>& up,
+                            const std::vector<uint32_t>& uo) {
+    c->pu_ok32 = c->pu_ok64 = false;
+    const char* path = getenv("FM_TRSV_PATH");
+    if (!path || std::strcmp(path, "push") != 0) return FM_OK;
+    constexpr uint32_t kCluster = 8;
+    constexpr size_t kMaxSmem = 227 * 1024;
+    auto env = [](const char* name, int dflt, int lo_, int hi) {
+        const char* v = getenv(name);
+        return v ? std::min(hi, std::max(lo_, atoi(v))) : dflt;
+    };
+    const int warps = env("FM_TRSV_PUSH_WARPS", 16, 1, 16);
+    const uint32_t block = (uint32_t)env("FM_TRSV_PUSH_BLOCK", 0, 0, 1 << 20);
+    const int nc32 = fm::push_max_clusters(4, kCluster, warps, kMaxSmem);
+    const int nc64 = fm::push_max_clusters(8, kCluster, warps, kMaxSmem);
+    const int ncl = std::min(nc32, nc64);
+    if (ncl < 1) return FM_OK;
+    fm::PushPlan p;
+    if (!fm::push_plan(c->graph, lp, lo, up, uo, (uint32_t)ncl, kCluster, block,
+                       (uint32_t)(kMaxSmem / fm::push_smem_bytes(1, 8)), p) &&
+        !fm::push_plan(c->graph, lp, lo, up, uo, (uint32_t)ncl, kCluster, block,
+                       (uint32_t)(kMaxSmem / fm::push_smem_bytes(1, 4)), p))
+        return FM_OK;
+    auto fits = [&](size_t vb) {
+        return fm::push_smem_bytes(std::max(p.max_slot_f, p.max_slot_b), vb) <= kMaxSmem;
+    };
+    const bool ok32 = fits(4), ok64 = fits(8);
+    if (!ok32 && !ok64) return FM_OK;
+    auto records = [&](const std::vector<uint32_t>& ord) {
+        std::vector<uint4> rec(ord.size());
+        for (size_t t = 0; t < ord.size(); ++t) {
+            const uint32_t nd = ord[t];
+            rec[t] = nd == ~0u ? make_uint4(~0u, 0, 0, 0)
+                               : make_uint4(nd, c->graph.ptr[nd],
+                                            c->graph.ptr[nd + 1] - c->graph.ptr[nd],
+                                            c->graph.self[nd]);
+        }
+        return rec;
+    };
+    const std::vector<uint4> rf = records(p.order_f), rb = records(p.order_b);
+    CK(upload(c->pu_pos_f, p.pos_f.data(), p.pos_f.size(), c->stream));
+    CK(upload(c->pu_pos_b, p.pos_b.data(), p.pos_b.size(), c->stream));
+    CK(upload(c->pu_src, p.src.data(), p.src.size(), c->stream));
+    CK(upload(c->pu_push_f, p.push_f.data(), p.push_f.size(), c->stream));
+    CK(upload(c->pu_push_b, p.push_b.data(), p.push_b.size(), c->stream));
+    CK(upload(c->pu_nslot_f, p.nslot_f.data(), p.nslot_f.size(), c->stream));
+    CK(upload(c->pu_nslot_b, p.nslot_b.data(), p.nslot_b.size(), c->stream));
+    CK(upload(c->pu_rec_f, rf.data(), rf.size(), c->stream));
+    CK(upload(c->pu_rec_b, rb.data(), rb.size(), c->stream));
+    fm::PushSolve v;
+    v.n_ctas = p.n_ctas;
+    v.cluster = p.cluster;
+    v.warps = (uint32_t)warps;
+    v.max_slot_f = p.max_slot_f;
+    v.max_slot_b = p.max_slot_b;
+    v.pos_f = c->pu_pos_f.p;
+    v.pos_b = c->pu_pos_b.p;
+    v.rec_f = c->pu_rec_f.p;
+    v.rec_b = c->pu_rec_b.p;
+    v.src = c->pu_src.p;
+    v.push_f = c->pu_push_f.p;
+    v.push_b = c->pu_push_b.p;
+    v.nslot_f = c->pu_nslot_f.p;
+    v.nslot_b = c->pu_nslot_b.p;
+    c->pu = v;
+    c->pu_ok32 = ok32;
+    c->pu_ok64 = ok64;
+    CK(cudaStreamSynchronize(c->stream));
+    return FM_OK;
+}
+
 // Plans for the one-lane-per-node cluster solves (fm_trsv_lanes.cu): a
 // 16-CTA cluster of 6 warps each; every level's groups of 32 nodes must fit
 // the cluster's warps once, and the neighbours per side the lane limit.
@@ -555,6 +639,15 @@ DevBuf<unsigned char>& packed_cards(fm_ctx* c, bool fwd);
 template <typename T>
 int precond_nodes(fm_ctx* c, const T* lu, const T* dinv, const T* r, T* tmp, T* z,
                   unsigned* status) {
+    const bool pu = sizeof(T) == 4 ? c->pu_ok32 : c->pu_ok64;
+    if (pu && c->nn) {
+        const cudaError_t e =
+            fm::launch_trsv_push<T>(c->pu, node_sched(c), lu, dinv, r, tmp, z, status, c->stream);
+        if (e == cudaSuccess) return z != r ? 3 : 4;
+        // a launch the device refuses: the pipelined solves from now on
+        cudaGetLastError();
+        c->pu_ok32 = c->pu_ok64 = false;
+    }
     const bool cl = sizeof(T) == 4 ? c->cl_ok32 : c->cl_ok64;
     if (cl && c->nn) {
         const cudaError_t e =
@@ -597,8 +690,9 @@ struct Op {
                                    c->stream);
     }
     void precond(const T* r, T* z) const {
+        const bool pu = node_block && (sizeof(T) == 4 ? c->pu_ok32 : c->pu_ok64);
         const bool cl = node_block && (sizeof(T) == 4 ? c->cl_ok32 : c->cl_ok64);
-        PROF(FM_PROF_TRSV, node_block && !cl ? 4 : 2);
+        PROF(FM_PROF_TRSV, pu ? (r != z ? 3 : 4) : node_block && !cl ? 4 : 2);
         if (node_block) {
             precond_nodes<T>(c, LU, dinv, r, tmp, z, c->status());
             return;
@@ -893,6 +987,7 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
             CK(upload(c->node_fwd_rec, rf.data(), rf.size(), c->stream));
             CK(upload(c->node_bwd_rec, rb.data(), rb.size(), c->stream));
             TRY(setup_cluster_solves(c, lp, lo, up, uo));
+            TRY(setup_push_solves(c, lp, lo, up, uo));
             CK(cudaStreamSynchronize(c->stream));
             CK(c->done.reserve(std::max<size_t>(c->done.n, (size_t)c->nn + 1)));
             CK(cudaMemsetAsync(c->done.p, 0, c->done.n * sizeof(unsigned), c->stream));

@@ -123,5 +123,45 @@ __device__ __forceinline__ void st_slot(uint32_t addr, T a, T b, T c) {
     st_val(addr + sizeof(T), b);
     st_val(addr + 2 * sizeof(T), c);
 }
+// A slot of this CTA's own shared memory, polled by its reader while a
+// CTA of the cluster (possibly this one) writes it with st_slot_cluster.
+template <typename T>
+__device__ __forceinline__ void ld_slot_cta(uint32_t addr, T& a, T& b, T& c);
+template <>
+__device__ __forceinline__ void ld_slot_cta<float>(uint32_t addr, float& a, float& b, float& c) {
+    [[maybe_unused]] float d;
+    asm volatile("ld.relaxed.cluster.shared::cta.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(a), "=f"(b), "=f"(c), "=f"(d)
+                 : "r"(addr)
+                 : "memory");
+}
+template <>
+__device__ __forceinline__ void ld_slot_cta<double>(uint32_t addr, double& a, double& b,
+                                                    double& c) {
+    [[maybe_unused]] double d;
+    asm volatile("ld.relaxed.cluster.shared::cta.v2.f64 {%0, %1}, [%2];"
+                 : "=d"(a), "=d"(b)
+                 : "r"(addr)
+                 : "memory");
+    asm volatile("ld.relaxed.cluster.shared::cta.v2.f64 {%0, %1}, [%2];"
+                 : "=d"(c), "=d"(d)
+                 : "r"(addr + 16)
+                 : "memory");
+}
+// The three values into a slot of any CTA of the cluster (addr from mapa);
+// the fourth word of the slot is padding.
+__device__ __forceinline__ void st_slot_cluster(uint32_t addr, float a, float b, float c) {
+    asm volatile("st.relaxed.cluster.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr),
+                 "f"(a), "f"(b), "f"(c), "f"(0.f)
+                 : "memory");
+}
+__device__ __forceinline__ void st_slot_cluster(uint32_t addr, double a, double b, double c) {
+    asm volatile("st.relaxed.cluster.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(addr), "d"(a),
+                 "d"(b)
+                 : "memory");
+    asm volatile("st.relaxed.cluster.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(addr + 16),
+                 "d"(c), "d"(0.0)
+                 : "memory");
+}
 }  // namespace clu
 }  // namespace fm

@@ -90,4 +90,34 @@ cudaError_t launch_trsv_cluster(const ClusterSolve& F, const ClusterSolve& B,
                                 const unsigned char* packed_f, const unsigned char* packed_b,
                                 const T* r, T* tmp, T* y, unsigned* status, cudaStream_t s);
 
+// Slab-partitioned push solves (fm_trsv_push.cu) on the plan of
+// fm_setup.cpp push_plan: CTA g of the grid (clusters of `cluster` CTAs)
+// walks positions pos_*[g] .. pos_*[g+1] of rec_* ({node, first neighbour
+// entry, degree, self position}; node ~0u: a hole), half-warp v every
+// (2 warps)-th of them from the v-th.
+struct PushSolve {
+    uint32_t n_ctas = 0, cluster = 0, warps = 0;
+    uint32_t max_slot_f = 0, max_slot_b = 0;
+    const uint32_t* pos_f = nullptr;
+    const uint32_t* pos_b = nullptr;
+    const uint4* rec_f = nullptr;
+    const uint4* rec_b = nullptr;
+    const uint32_t* src = nullptr;     // per neighbour entry: reader-side slot or ~0u
+    const uint32_t* push_f = nullptr;  // 8 per node: rank << 20 | slot, ~0u after the last
+    const uint32_t* push_b = nullptr;
+    const uint32_t* nslot_f = nullptr;  // slots per CTA
+    const uint32_t* nslot_b = nullptr;
+};
+// dynamic shared memory of one CTA of a direction with max_slot slots
+size_t push_smem_bytes(uint32_t max_slot, size_t value_bytes);
+// clusters of `cluster` CTAs (warps each, smem bytes) that can be resident
+// at once for both directions' kernels of this value width (0: none)
+int push_max_clusters(size_t value_bytes, int cluster, int warps, size_t smem);
+// y = U^-1 L^-1 r through tmp (three kernels: tmp's sentinel fill, the
+// forward solve, which also fills y unless y aliases r, and the backward);
+// returns the first launch error, with nothing left half-done on success
+template <typename T>
+cudaError_t launch_trsv_push(const PushSolve& P, const NodeSched& S, const T* lu, const T* dinv,
+                             const T* r, T* tmp, T* y, unsigned* status, cudaStream_t s);
+
 }  // namespace fm

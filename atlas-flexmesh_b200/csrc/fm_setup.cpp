@@ -262,6 +262,113 @@ bool cluster_plan(const NodeGraph& g, bool lower, const std::vector<uint32_t>& p
     return true;
 }
 
+bool push_plan(const NodeGraph& g, const std::vector<uint32_t>& fwd_ptr,
+               const std::vector<uint32_t>& fwd_order, const std::vector<uint32_t>& bwd_ptr,
+               const std::vector<uint32_t>& bwd_order, uint32_t n_clusters, uint32_t cluster,
+               uint32_t block, uint32_t max_slots, PushPlan& plan) {
+    const uint32_t nn = g.n_nodes;
+    plan = PushPlan();
+    if (!nn || !n_clusters || !cluster || cluster > kPushMax || fwd_order.size() != nn ||
+        bwd_order.size() != nn || fwd_ptr.size() < 2 || bwd_ptr.size() < 2)
+        return false;
+    const uint32_t nc = n_clusters * cluster;
+    const uint32_t nlf = (uint32_t)fwd_ptr.size() - 1, nlb = (uint32_t)bwd_ptr.size() - 1;
+    std::vector<uint32_t> lf(nn), lb(nn);
+    for (uint32_t l = 0; l < nlf; ++l)
+        for (uint32_t t = fwd_ptr[l]; t < fwd_ptr[l + 1]; ++t) lf[fwd_order[t]] = l;
+    for (uint32_t l = 0; l < nlb; ++l)
+        for (uint32_t t = bwd_ptr[l]; t < bwd_ptr[l + 1]; ++t) lb[bwd_order[t]] = l;
+    // busiest CTA's share of one level, either direction
+    std::vector<uint32_t> cf((size_t)nc * nlf), cb((size_t)nc * nlb);
+    auto share = [&](uint32_t R) {
+        std::fill(cf.begin(), cf.end(), 0u);
+        std::fill(cb.begin(), cb.end(), 0u);
+        uint32_t mx = 0;
+        for (uint32_t n = 0; n < nn; ++n) {
+            const uint32_t c = push_cta(n, nn, n_clusters, cluster, R);
+            mx = std::max(mx, ++cf[(size_t)c * nlf + lf[n]]);
+            mx = std::max(mx, ++cb[(size_t)c * nlb + lb[n]]);
+        }
+        return mx;
+    };
+    std::vector<std::pair<uint32_t, uint32_t>> cand;  // (share, block)
+    if (block) {
+        cand.push_back({share(block), block});
+    } else {
+        for (uint32_t R = 16; R <= 512; R += R < 128 ? 1 : 8) cand.push_back({share(R), R});
+        std::sort(cand.begin(), cand.end());
+    }
+    std::vector<uint32_t> cta(nn);
+    auto slots = [&](bool lower, std::vector<uint32_t>& push, std::vector<uint32_t>& nslot,
+                     uint32_t& max_slot) {
+        push.assign((size_t)nn * kPushMax, ~0u);
+        nslot.assign(nc, 0);
+        std::vector<uint8_t> npush(nn, 0);
+        for (uint32_t s = 0; s < n_clusters; ++s) {
+            const uint32_t b = push_slab_begin(s, nn, n_clusters);
+            const uint32_t e = push_slab_begin(s + 1, nn, n_clusters);
+            // slot of producer m in the slab's CTA of rank r: slot[(m - b) * cluster + r]
+            std::vector<uint32_t> slot((size_t)(e - b) * cluster, ~0u);
+            for (uint32_t n = b; n < e; ++n) {
+                const uint32_t c = cta[n], r = c - s * cluster;
+                uint32_t cnt = 0;
+                for (uint32_t k = g.ptr[n]; k < g.ptr[n + 1]; ++k) {
+                    const uint32_t m = g.nbr[k];
+                    if (m == n || (m < n) != lower) continue;
+                    ++cnt;
+                    if (m < b || m >= e) continue;  // another slab: through global memory
+                    uint32_t& sl = slot[(size_t)(m - b) * cluster + r];
+                    if (sl == ~0u) {
+                        sl = nslot[c]++;
+                        if (sl >= max_slots) return false;
+                        push[(size_t)m * kPushMax + npush[m]++] = r << 20 | sl;
+                    }
+                    plan.src[k] = sl;
+                }
+                if (cnt > 16) return false;
+            }
+        }
+        max_slot = *std::max_element(nslot.begin(), nslot.end());
+        return true;
+    };
+    max_slots = std::min(max_slots, 1u << 20);
+    for (const auto& cs : cand) {
+        const uint32_t R = cs.second;
+        for (uint32_t n = 0; n < nn; ++n) cta[n] = push_cta(n, nn, n_clusters, cluster, R);
+        plan.src.assign(g.nbr.size(), ~0u);
+        if (!slots(true, plan.push_f, plan.nslot_f, plan.max_slot_f) ||
+            !slots(false, plan.push_b, plan.nslot_b, plan.max_slot_b))
+            continue;
+        plan.n_ctas = nc;
+        plan.cluster = cluster;
+        plan.block = R;
+        plan.max_level_share = cs.first;
+        // each CTA's nodes keep the relative order of the global level order;
+        // a level that would start at an odd position of its CTA gets a hole first
+        auto split = [&](const std::vector<uint32_t>& order, const std::vector<uint32_t>& lev,
+                         std::vector<uint32_t>& pos, std::vector<uint32_t>& out) {
+            std::vector<std::vector<uint32_t>> per(nc);
+            for (uint32_t n : order) {
+                std::vector<uint32_t>& v = per[cta[n]];
+                if ((v.size() & 1) && lev[v.back()] != lev[n]) v.push_back(~0u);
+                v.push_back(n);
+            }
+            pos.assign(nc + 1, 0);
+            out.clear();
+            for (uint32_t c = 0; c < nc; ++c) {
+                if (per[c].size() & 1) per[c].push_back(~0u);
+                out.insert(out.end(), per[c].begin(), per[c].end());
+                pos[c + 1] = (uint32_t)out.size();
+            }
+        };
+        split(fwd_order, lf, plan.pos_f, plan.order_f);
+        split(bwd_order, lb, plan.pos_b, plan.order_b);
+        return true;
+    }
+    plan = PushPlan();
+    return false;
+}
+
 void ilu_edge_maps(const NodeGraph& g, std::vector<uint32_t>& ptr, std::vector<uint8_t>& map) {
     const uint32_t n = g.n_nodes;
     ptr.assign(n + 1, 0);

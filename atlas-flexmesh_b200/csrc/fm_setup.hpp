@@ -109,6 +109,64 @@ bool cluster_plan(const NodeGraph& g, bool lower, const std::vector<uint32_t>& p
 // it.  Neighbour lists hold at most 32 nodes, so a position fits a byte.
 void ilu_edge_maps(const NodeGraph& g, std::vector<uint32_t>& ptr, std::vector<uint8_t>& map);
 
+// Plan of the slab-partitioned push solves (fm_trsv_push.cu).  The node
+// range is cut into n_clusters contiguous slabs, one per thread-block
+// cluster of `cluster` CTAs.  Both solves only ever wait on nodes on one
+// side in the numbering (lower for the forward, upper for the backward), so
+// a chain of dependencies leaves a slab at most n_clusters - 1 times: every
+// other dependency hop stays inside one cluster.  There the producer stores
+// its three values into a shared-memory slot of each CTA that reads them
+// (one slot per producer and reading CTA, no reuse), and the readers poll
+// their own shared memory; across slabs values go through global memory as
+// in the grid-wide solves.  Inside a slab, blocks of `block` consecutive
+// nodes are dealt round-robin to the cluster's CTAs, so that every CTA holds
+// a share of each level (block is chosen to keep the busiest CTA's share of
+// any level small).
+constexpr uint32_t kPushMax = 8;  // reading CTAs per producer, at most (= cluster size)
+struct PushPlan {
+    uint32_t n_ctas = 0, cluster = 0, block = 0;
+    uint32_t max_level_share = 0;  // most nodes of one level in one CTA
+    // CTA g's nodes are positions pos_f[g] .. pos_f[g + 1] of order_f (and
+    // likewise backward), sorted by that direction's level and padded with
+    // holes (~0u) so that positions 2i and 2i + 1 of a CTA, which one warp
+    // resolves together, are never two nodes of different levels
+    std::vector<uint32_t> pos_f, pos_b;  // n_ctas + 1 each
+    std::vector<uint32_t> order_f, order_b;
+    // per neighbour entry e of node n (graph order): the neighbour's slot in
+    // n's CTA when the neighbour is on the solve's side and in n's slab, else
+    // ~0u (read from global memory).  Lower entries serve the forward solve,
+    // upper ones the backward; the self entry is ~0u.
+    std::vector<uint32_t> src;
+    // kPushMax per node and direction: rank << 20 | slot of each reading CTA
+    // of the node's slab, ~0u after the last
+    std::vector<uint32_t> push_f, push_b;
+    std::vector<uint32_t> nslot_f, nslot_b;  // slots per CTA
+    uint32_t max_slot_f = 0, max_slot_b = 0;
+};
+
+// CTA of node n: its slab's first CTA plus the round-robin rank of its block
+// (slab s holds nodes ceil(s n_nodes / n_clusters) .. ceil((s+1) n_nodes / n_clusters) - 1)
+FM_HD inline uint32_t push_slab_begin(uint32_t s, uint32_t n_nodes, uint32_t n_clusters) {
+    return (uint32_t)(((uint64_t)s * n_nodes + n_clusters - 1) / n_clusters);
+}
+FM_HD inline uint32_t push_cta(uint32_t n, uint32_t n_nodes, uint32_t n_clusters,
+                               uint32_t cluster, uint32_t block) {
+    const uint32_t s = (uint32_t)((uint64_t)n * n_clusters / n_nodes);
+    return s * cluster + ((n - push_slab_begin(s, n_nodes, n_clusters)) / block) % cluster;
+}
+
+// Builds the plan for n_clusters clusters of `cluster` CTAs (cluster <=
+// kPushMax) from the level orders and level pointers of node_levels.  block
+// = 0 picks the block size in 16 .. 512 with the smallest busiest-CTA level
+// share whose slot counts stay within max_slots (ties: the smaller size).
+// Returns false when a side of some node has more than 16 neighbours (the
+// solves give each node a half-warp) or no block size keeps the slots
+// within max_slots.
+bool push_plan(const NodeGraph& g, const std::vector<uint32_t>& fwd_ptr,
+               const std::vector<uint32_t>& fwd_order, const std::vector<uint32_t>& bwd_ptr,
+               const std::vector<uint32_t>& bwd_order, uint32_t n_clusters, uint32_t cluster,
+               uint32_t block, uint32_t max_slots, PushPlan& plan);
+
 // Cards of the cluster solves are ordered by (level, warp, node): position
 // level_start + gw + j W of a level of `width` positions is warp gw's j-th
 // node there, and warp gw holds q + (gw < r) of the level's cards
