@@ -394,25 +394,28 @@ fm::NodeSched node_sched(const fm_ctx* c) {
 // Plan of the slab-partitioned push solves (fm_trsv_push.cu): one slab per
 // cluster of 8 CTAs, as many clusters as the device keeps resident (FP32 and
 // FP64 kernels alike), when every CTA's slots fit its shared memory (the
-// plan first tries to fit FP64 slots, else FP32 only).  Selected with
-// FM_TRSV_PATH=push; FM_TRSV_PUSH_WARPS sets the warps per CTA (default 16),
-// FM_TRSV_PUSH_BLOCK the interleave block (default: chosen by the plan).
+// plan first tries to fit FP64 slots, else FP32 only) and no node has more
+// than 16 neighbours on a side.  The default path; FM_TRSV_PATH=pipe (or a
+// cluster path) selects another.  FM_TRSV_PUSH_WARPS caps the warps per CTA
+// (default: 24 in FP32, 16 in FP64), FM_TRSV_PUSH_BLOCK sets the interleave
+// block (default: chosen by the plan).
 fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
                             const std::vector<uint32_t>& lo, const std::vector<uint32_t>& up,
                             const std::vector<uint32_t>& uo) {
     c->pu_ok32 = c->pu_ok64 = false;
     const char* path = getenv("FM_TRSV_PATH");
-    if (!path || std::strcmp(path, "push") != 0) return FM_OK;
+    if (path && std::strcmp(path, "push") != 0) return FM_OK;
     constexpr uint32_t kCluster = 8;
     constexpr size_t kMaxSmem = 227 * 1024;
     auto env = [](const char* name, int dflt, int lo_, int hi) {
         const char* v = getenv(name);
         return v ? std::min(hi, std::max(lo_, atoi(v))) : dflt;
     };
-    const int warps = env("FM_TRSV_PUSH_WARPS", 16, 1, 16);
+    const int warps32 = env("FM_TRSV_PUSH_WARPS", fm::push_max_warps(4), 1, fm::push_max_warps(4));
+    const int warps64 = std::min(warps32, fm::push_max_warps(8));
     const uint32_t block = (uint32_t)env("FM_TRSV_PUSH_BLOCK", 0, 0, 1 << 20);
-    const int nc32 = fm::push_max_clusters(4, kCluster, warps, kMaxSmem);
-    const int nc64 = fm::push_max_clusters(8, kCluster, warps, kMaxSmem);
+    const int nc32 = fm::push_max_clusters(4, kCluster, warps32, kMaxSmem);
+    const int nc64 = fm::push_max_clusters(8, kCluster, warps64, kMaxSmem);
     const int ncl = std::min(nc32, nc64);
     if (ncl < 1) return FM_OK;
     fm::PushPlan p;
@@ -450,7 +453,8 @@ fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
     fm::PushSolve v;
     v.n_ctas = p.n_ctas;
     v.cluster = p.cluster;
-    v.warps = (uint32_t)warps;
+    v.warps32 = (uint32_t)warps32;
+    v.warps64 = (uint32_t)warps64;
     v.max_slot_f = p.max_slot_f;
     v.max_slot_b = p.max_slot_b;
     v.pos_f = c->pu_pos_f.p;

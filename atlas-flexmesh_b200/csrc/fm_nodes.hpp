@@ -96,7 +96,7 @@ cudaError_t launch_trsv_cluster(const ClusterSolve& F, const ClusterSolve& B,
 // entry, degree, self position}; node ~0u: a hole), half-warp v every
 // (2 warps)-th of them from the v-th.
 struct PushSolve {
-    uint32_t n_ctas = 0, cluster = 0, warps = 0;
+    uint32_t n_ctas = 0, cluster = 0, warps32 = 0, warps64 = 0;  // warps per CTA
     uint32_t max_slot_f = 0, max_slot_b = 0;
     const uint32_t* pos_f = nullptr;
     const uint32_t* pos_b = nullptr;
@@ -108,6 +108,8 @@ struct PushSolve {
     const uint32_t* nslot_f = nullptr;  // slots per CTA
     const uint32_t* nslot_b = nullptr;
 };
+// most warps per CTA of the push kernels of this value width (register budget)
+constexpr int push_max_warps(size_t value_bytes) { return value_bytes == 4 ? 24 : 16; }
 // dynamic shared memory of one CTA of a direction with max_slot slots
 size_t push_smem_bytes(uint32_t max_slot, size_t value_bytes);
 // clusters of `cluster` CTAs (warps each, smem bytes) that can be resident

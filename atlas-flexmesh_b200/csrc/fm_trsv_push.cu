@@ -6,10 +6,12 @@
 // N^3 block); in the grid-wide solves (fm_trsv.cu) every hop of the chain
 // is a value stored to L2 and polled back by another SM, ~0.43 us of the
 // ~0.92 us a level costs.  Here the node range is cut into one contiguous
-// slab per cluster (8 CTAs, one per SM) and each slab into one range per
-// CTA.  The forward solve only waits on lower-numbered nodes and the
-// backward on higher-numbered ones, so any dependency chain leaves a slab
-// at most (clusters - 1) times; every other hop stays inside a cluster:
+// slab per cluster (8 CTAs, one per SM), whose blocks of consecutive nodes
+// are dealt round-robin to the cluster's CTAs (so that each CTA holds a
+// share of every level).  The forward solve only waits on lower-numbered
+// nodes and the backward on higher-numbered ones, so any dependency chain
+// leaves a slab at most (clusters - 1) times; every other hop stays inside
+// a cluster:
 //
 //   * the producing warp stores the node's three values, with one relaxed
 //     cluster-scope vector store per reading CTA, into a slot of that CTA's
@@ -21,12 +23,24 @@
 //     precedes every push, and a second barrier keeps every CTA resident
 //     until no store into its shared memory can still be in flight.
 //
-// Per warp the schedule is the grid-wide one: positions of its CTA in level
-// order, warp w taking every warps-th, the next node's record, LU blocks and
-// destinations in flight while it waits; lane k owns neighbour k on the
-// solve's side and the waits run in lock step, ending in a butterfly that
-// leaves the sums in every lane.  The per-node arithmetic is that of
-// fm_trsv.cu term for term, so both paths give the same bits.
+// Each CTA walks its nodes in level order; a warp resolves two nodes at a
+// time, one per half-warp, and lane k of a half owns the node's k-th
+// neighbour on the solve's side (at most 16; meshes with more keep the
+// grid-wide solves).  The host pads every CTA's level runs with holes so
+// that the two nodes of a warp never belong to different levels: neither
+// then waits on the other, and the waits of both halves run in lock step
+// (one warp vote), ending in butterflies inside each half.  The next pair's
+// records (batched 16 per half-warp, a batch ahead, handed out by
+// shuffles), LU blocks, slots and destinations are in flight while the
+// warp waits.  The per-node arithmetic is that of fm_trsv.cu term for term
+// (lanes without a neighbour add zeros), so both paths give the same values.
+//
+// Measured on B200 at 64^3 x 6 tets, FP32 (per forward+backward pair):
+// 0.716 ms grid-wide, 0.492 ms here with 24 warps per CTA (FP64: 0.806 ->
+// 0.710 ms with 16).  A per-node %globaltimer trace put the in-cluster hop
+// at 128 ns median against 480 ns through L2, and showed a build with one
+// node per warp bound by the warps' own per-node work (0.83 us issuing the
+// next node's loads); two nodes per warp halved that work per node.
 //
 // The backward solve runs its slabs in reverse block order (the top slab on
 // the first clusters), so in both directions clusters only wait on clusters
@@ -211,7 +225,7 @@ __device__ __forceinline__ uint4 shfl4(uint4 v, int src) {
 // sentinel once its CTA is done (the forward solve prepares the backward's
 // output this way).
 template <typename T, bool Lower>
-__global__ void __launch_bounds__(16 * 32, 1)
+__global__ void __launch_bounds__(push_max_warps(sizeof(T)) * 32, 1)
     k_trsv_push(PushSolve P, NodeSched S, const T* __restrict__ lu, const T* __restrict__ dinv,
                 const T* __restrict__ rhs, T* __restrict__ out, T* __restrict__ fill,
                 uint32_t n_fill, unsigned* __restrict__ status) {
@@ -315,7 +329,7 @@ static cudaError_t launch_dir(const PushSolve& P, const NodeSched& S, const T* l
                               cudaStream_t s) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(P.n_ctas);
-    cfg.blockDim = dim3(32 * P.warps);
+    cfg.blockDim = dim3(32 * (sizeof(T) == 4 ? P.warps32 : P.warps64));
     cfg.dynamicSmemBytes = push_smem_bytes(Lower ? P.max_slot_f : P.max_slot_b, sizeof(T));
     cfg.stream = s;
     cudaLaunchAttribute at[1];
@@ -336,7 +350,9 @@ size_t push_smem_bytes(uint32_t max_slot, size_t value_bytes) {
 }
 
 int push_max_clusters(size_t value_bytes, int cluster, int warps, size_t smem) {
-    if (warps < 1 || warps > 16 || cluster < 1 || cluster > (int)kPushMax) return 0;
+    if (warps < 1 || warps > push_max_warps(value_bytes) || cluster < 1 ||
+        cluster > (int)kPushMax)
+        return 0;
     // raises each kernel's dynamic shared memory limit to smem, so every later
     // launch up to that size is accepted
     if (value_bytes == 4)

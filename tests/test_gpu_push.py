@@ -1,5 +1,5 @@
-"""The slab-partitioned push solves (FM_TRSV_PATH=push, fm_trsv_push.cu)
-against the grid-wide pipelined solves (fm_trsv.cu).
+"""The slab-partitioned push solves (fm_trsv_push.cu, the default path)
+against the grid-wide pipelined solves (fm_trsv.cu, FM_TRSV_PATH=pipe).
 
 Both walk the same node-block factors with the same per-node arithmetic
 (lane k owns neighbour k, the same butterfly, the same finish), so every
@@ -66,10 +66,7 @@ def block(N, seed):
 
 def context(fm, monkeypatch, mesh, push):
     P, xyz, conn, mask, val = mesh
-    if push:
-        monkeypatch.setenv("FM_TRSV_PATH", "push")
-    else:
-        monkeypatch.delenv("FM_TRSV_PATH", raising=False)
+    monkeypatch.setenv("FM_TRSV_PATH", "push" if push else "pipe")
     ctx = fm.Context(0)
     ctx.set_mesh(xyz, conn, P.elem_volume)
     monkeypatch.delenv("FM_TRSV_PATH", raising=False)
