@@ -272,6 +272,26 @@ bool push_plan(const NodeGraph& g, const std::vector<uint32_t>& fwd_ptr,
         bwd_order.size() != nn || fwd_ptr.size() < 2 || bwd_ptr.size() < 2)
         return false;
     const uint32_t nc = n_clusters * cluster;
+    max_slots = std::min(max_slots, 1u << 20);
+    // Every node read inside its own slab takes at least one slot in some
+    // CTA of the slab, so a slab with more such nodes than cluster *
+    // max_slots cannot fit with any block size: refuse before the search.
+    for (int lower = 1; lower >= 0; --lower) {
+        for (uint32_t s = 0; s < n_clusters; ++s) {
+            const uint32_t b = push_slab_begin(s, nn, n_clusters);
+            const uint32_t e = push_slab_begin(s + 1, nn, n_clusters);
+            uint64_t read = 0;
+            for (uint32_t m = b; m < e; ++m)
+                for (uint32_t k = g.ptr[m]; k < g.ptr[m + 1]; ++k) {
+                    const uint32_t n = g.nbr[k];  // a reader of m on this side?
+                    if (n >= b && n < e && (lower ? n > m : n < m)) {
+                        ++read;
+                        break;
+                    }
+                }
+            if (read > (uint64_t)cluster * max_slots) return false;
+        }
+    }
     const uint32_t nlf = (uint32_t)fwd_ptr.size() - 1, nlb = (uint32_t)bwd_ptr.size() - 1;
     std::vector<uint32_t> lf(nn), lb(nn);
     for (uint32_t l = 0; l < nlf; ++l)
@@ -331,7 +351,6 @@ bool push_plan(const NodeGraph& g, const std::vector<uint32_t>& fwd_ptr,
         max_slot = *std::max_element(nslot.begin(), nslot.end());
         return true;
     };
-    max_slots = std::min(max_slots, 1u << 20);
     for (const auto& cs : cand) {
         const uint32_t R = cs.second;
         for (uint32_t n = 0; n < nn; ++n) cta[n] = push_cta(n, nn, n_clusters, cluster, R);
