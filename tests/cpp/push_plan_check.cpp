@@ -19,7 +19,11 @@
 //     neighbour's push list names it (reader rank, slot);
 //   * every push list entry is read by some entry, lists are terminated
 //     by ~0u and hold no duplicates; entries off the solve's side are ~0u
-//     for the side's own walk.
+//     for the side's own walk;
+//   * the kernels' schedule cannot deadlock: with W warps per CTA, warp w
+//     resolves positions (2w + qH, 2w + 1 + qH), H = 2W, q = 0, 1, ... of
+//     its CTA in order, a pair only once every dependency of both nodes is
+//     resolved; simulated to a fixpoint for several W, every node resolves.
 // Prints "ok" and exits 0, or names the first violation and exits 1.
 #include <algorithm>
 #include <cstdio>
@@ -162,6 +166,42 @@ int main(int argc, char** argv) {
                     }
                 if (!found) return fail("producer does not push to its reader", m, n);
             }
+        }
+        // schedule simulation: every warp advances while its next pair is ready
+        for (uint32_t W : {1u, 3u, 16u, 24u}) {
+            const uint32_t H = 2 * W;
+            std::vector<uint8_t> done(nn, 0);
+            std::vector<uint32_t> q((size_t)nc * W, 0);
+            auto ready = [&](uint32_t t) {
+                const uint32_t n = ord[t];
+                if (n == ~0u) return true;
+                for (uint32_t k = g.ptr[n]; k < g.ptr[n + 1]; ++k) {
+                    const uint32_t m = g.nbr[k];
+                    if (m != n && (m < n) == (lower != 0) && !done[m]) return false;
+                }
+                return true;
+            };
+            uint32_t resolved = 0;
+            for (bool moved = true; moved;) {
+                moved = false;
+                for (uint32_t c = 0; c < nc; ++c)
+                    for (uint32_t w = 0; w < W; ++w) {
+                        uint32_t& qq = q[(size_t)c * W + w];
+                        for (;;) {
+                            const uint32_t t = pos[c] + 2 * w + qq * H;
+                            if (t >= pos[c + 1]) break;
+                            if (!ready(t) || !ready(t + 1)) break;
+                            for (uint32_t u : {t, t + 1})
+                                if (ord[u] != ~0u) {
+                                    done[ord[u]] = 1;
+                                    ++resolved;
+                                }
+                            ++qq;
+                            moved = true;
+                        }
+                    }
+            }
+            if (resolved != nn) return fail("schedule deadlocks", W, resolved);
         }
         for (uint32_t m = 0; m < nn; ++m) {
             bool ended = false;
