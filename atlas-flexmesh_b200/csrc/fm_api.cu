@@ -391,6 +391,18 @@ fm::NodeSched node_sched(const fm_ctx* c) {
     return S;
 }
 
+// The 16-byte schedule record {node, first neighbour entry, degree, self
+// position} of every position of a node order; a hole (~0u) gets node ~0u.
+static std::vector<uint4> node_records(const fm::NodeGraph& g, const std::vector<uint32_t>& ord) {
+    std::vector<uint4> rec(ord.size());
+    for (size_t t = 0; t < ord.size(); ++t) {
+        const uint32_t nd = ord[t];
+        rec[t] = nd == ~0u ? make_uint4(~0u, 0, 0, 0)
+                           : make_uint4(nd, g.ptr[nd], g.ptr[nd + 1] - g.ptr[nd], g.self[nd]);
+    }
+    return rec;
+}
+
 // Plan of the slab-partitioned push solves (fm_trsv_push.cu): one slab per
 // cluster of 8 CTAs, as many clusters as the device keeps resident (FP32 and
 // FP64 kernels alike), when every CTA's slots fit its shared memory (the
@@ -429,18 +441,8 @@ fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
     };
     const bool ok32 = fits(4), ok64 = fits(8);
     if (!ok32 && !ok64) return FM_OK;
-    auto records = [&](const std::vector<uint32_t>& ord) {
-        std::vector<uint4> rec(ord.size());
-        for (size_t t = 0; t < ord.size(); ++t) {
-            const uint32_t nd = ord[t];
-            rec[t] = nd == ~0u ? make_uint4(~0u, 0, 0, 0)
-                               : make_uint4(nd, c->graph.ptr[nd],
-                                            c->graph.ptr[nd + 1] - c->graph.ptr[nd],
-                                            c->graph.self[nd]);
-        }
-        return rec;
-    };
-    const std::vector<uint4> rf = records(p.order_f), rb = records(p.order_b);
+    const std::vector<uint4> rf = node_records(c->graph, p.order_f);
+    const std::vector<uint4> rb = node_records(c->graph, p.order_b);
     CK(upload(c->pu_pos_f, p.pos_f.data(), p.pos_f.size(), c->stream));
     CK(upload(c->pu_pos_b, p.pos_b.data(), p.pos_b.size(), c->stream));
     CK(upload(c->pu_src, p.src.data(), p.src.size(), c->stream));
@@ -978,16 +980,8 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
             CK(upload(c->node_fwd, lo.data(), lo.size(), c->stream));
             CK(upload(c->node_bwd, uo.data(), uo.size(), c->stream));
             // one 16-byte schedule record per position of each order
-            auto records = [&](const std::vector<uint32_t>& ord) {
-                std::vector<uint4> rec(ord.size());
-                for (size_t t = 0; t < ord.size(); ++t) {
-                    const uint32_t nd = ord[t];
-                    rec[t] = make_uint4(nd, c->graph.ptr[nd], c->graph.ptr[nd + 1] - c->graph.ptr[nd],
-                                        c->graph.self[nd]);
-                }
-                return rec;
-            };
-            const std::vector<uint4> rf = records(lo), rb = records(uo);
+            const std::vector<uint4> rf = node_records(c->graph, lo);
+            const std::vector<uint4> rb = node_records(c->graph, uo);
             CK(upload(c->node_fwd_rec, rf.data(), rf.size(), c->stream));
             CK(upload(c->node_bwd_rec, rb.data(), rb.size(), c->stream));
             TRY(setup_cluster_solves(c, lp, lo, up, uo));
