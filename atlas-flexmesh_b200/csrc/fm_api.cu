@@ -103,15 +103,6 @@ struct fm_ctx {
     DevBuf<uint8_t> emap;  // ILU(0) update map
     DevBuf<uint4> node_fwd_rec, node_bwd_rec;
     uint32_t node_levels_fwd = 0, node_levels_bwd = 0, width_fwd = 0, width_bwd = 0;
-    // cluster-synchronous solves (fm_trsv_cluster.cu): plans of both
-    // directions and whether the device runs them in FP32 / FP64
-    DevBuf<uint32_t> cl_lvl_f, cl_lvl_b, cl_nslot, cl_rptr_f, cl_rptr_b, cl_reset_f, cl_reset_b;
-    DevBuf<uint4> cl_rec_f, cl_rec_b;
-    DevBuf<uint32_t> cl_card_f, cl_card_b;  // card index of every position
-    DevBuf<unsigned char> cl_pack32_f, cl_pack32_b, cl_pack64_f, cl_pack64_b;
-    fm::ClusterSolve cl_f, cl_b;
-    bool cl_ok32 = false, cl_ok64 = false;
-    bool cl_lanes = false;  // one lane per node (fm_trsv_lanes.cu); cl_card_* = group starts
     std::vector<uint32_t> lvl_fwd_ptr, lvl_fwd_rows, lvl_bwd_ptr, lvl_bwd_rows;
     // slab-partitioned push solves (fm_trsv_push.cu): plan on the device and
     // whether they run in FP32 / FP64
@@ -160,6 +151,9 @@ struct fm_ctx {
     double prof_ms[FM_PROF_KINDS] = {};
     uint64_t prof_calls[FM_PROF_KINDS] = {};
     uint64_t prof_kernels[FM_PROF_KINDS] = {};
+
+    // per-solve records of the latest Newton call (fm_newton_history)
+    std::vector<fm_newton_record> newton_hist;
 
     unsigned* status() { return &sc.p->status; }
     unsigned* counter() { return &sc.p->counter[0]; }
@@ -225,9 +219,9 @@ struct ProfScope {
     int kind;
     cudaEvent_t a = nullptr;
     ProfScope(fm_ctx* ctx, int k, int kernels) : c(ctx), kind(k) {
-        if (!c->prof_on) return;
         c->prof_calls[k] += 1;
         c->prof_kernels[k] += (uint64_t)kernels;
+        if (!c->prof_on) return;
         a = prof_event(c);
         if (a) cudaEventRecord(a, c->stream);
     }
@@ -261,12 +255,27 @@ fm_status device_flags(fm_ctx* c, uint32_t* flags) {
     return FM_OK;
 }
 
+// The device flags as words, for error texts
+std::string flags_text(uint32_t f) {
+    static const char* names[] = {"nonfinite", "inverted", "J_clamped", "pivot_perturbed",
+                                  "timeout", "breakdown"};
+    std::string s;
+    for (int b = 0; b < 6; ++b)
+        if (f & (1u << b)) {
+            if (!s.empty()) s += ",";
+            s += names[b];
+        }
+    return s.empty() ? "none" : s;
+}
+
 // Translate fatal device flags into a status
 fm_status check_flags(fm_ctx* c, uint32_t flags, const char* where) {
     if (flags & FM_FLAG_TIMEOUT)
-        return fail(c, FM_ERR_TIMEOUT, "%s: a bounded dependency wait expired", where);
+        return fail(c, FM_ERR_TIMEOUT, "%s: a bounded dependency wait expired (flags: %s)", where,
+                    flags_text(flags).c_str());
     if (flags & FM_FLAG_NONFINITE)
-        return fail(c, FM_ERR_NONFINITE, "%s: non-finite value produced", where);
+        return fail(c, FM_ERR_NONFINITE, "%s: non-finite value produced (flags: %s)", where,
+                    flags_text(flags).c_str());
     return FM_OK;
 }
 
@@ -407,8 +416,8 @@ static std::vector<uint4> node_records(const fm::NodeGraph& g, const std::vector
 // cluster of 8 CTAs, as many clusters as the device keeps resident (FP32 and
 // FP64 kernels alike), when every CTA's slots fit its shared memory (the
 // plan first tries to fit FP64 slots, else FP32 only) and no node has more
-// than 16 neighbours on a side.  The default path; FM_TRSV_PATH=pipe (or a
-// cluster path) selects another.  FM_TRSV_PUSH_WARPS caps the warps per CTA
+// than 16 neighbours on a side.  The default path; FM_TRSV_PATH=pipe selects
+// the grid-wide pipelined solves (fm_trsv.cu) instead.  FM_TRSV_PUSH_WARPS caps the warps per CTA
 // (default: 24 in FP32, 16 in FP64), FM_TRSV_PUSH_BLOCK sets the interleave
 // block (default: chosen by the plan).
 fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
@@ -475,173 +484,9 @@ fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
     return FM_OK;
 }
 
-// Plans for the one-lane-per-node cluster solves (fm_trsv_lanes.cu): a
-// 16-CTA cluster of 6 warps each; every level's groups of 32 nodes must fit
-// the cluster's warps once, and the neighbours per side the lane limit.
-fm_status setup_lane_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
-                            const std::vector<uint32_t>& lo, const std::vector<uint32_t>& up,
-                            const std::vector<uint32_t>& uo) {
-    constexpr uint32_t kCs = 16, kWarps = 6, kMaxSlots = 4096;
-    constexpr size_t kMaxSmem = 227 * 1024;
-    const char* wenv = getenv("FM_TRSV_WINDOW");
-    const uint32_t window = wenv ? std::max(1u, (uint32_t)strtoul(wenv, nullptr, 10)) : 8u;
-    fm::ClusterPlan pf, pb;
-    std::vector<uint32_t> nslot;
-    if (!fm::cluster_plan(c->graph, true, lp, lo, kCs, kWarps, window, kMaxSlots, pf, nslot, true) ||
-        !fm::cluster_plan(c->graph, false, up, uo, kCs, kWarps, window, kMaxSlots, pb, nslot, true))
-        return FM_OK;
-    if (pf.max_per_warp > 1 || pb.max_per_warp > 1) return FM_OK;
-    if (pf.max_cnt > (uint32_t)fm::lanes_max_neighbours() ||
-        pb.max_cnt > (uint32_t)fm::lanes_max_neighbours())
-        return FM_OK;
-    auto view = [](const fm::ClusterPlan& p) {
-        fm::ClusterSolve v;
-        v.n_levels = p.n_levels;
-        v.n_ctas = p.n_ctas;
-        v.warps_per_cta = p.warps_per_cta;
-        v.max_per_warp = 1;
-        v.maxc = std::max(p.max_cnt, 1u);
-        v.pool_slots = std::max(p.slots_per_cta, 1u);
-        v.window = p.window;
-        v.n_groups = p.n_groups;
-        const char* sl = getenv("FM_TRSV_SLEEP_NS");
-        v.sleep_ns = sl ? (uint32_t)strtoul(sl, nullptr, 10) : 0u;
-        return v;
-    };
-    fm::ClusterSolve f = view(pf), b = view(pb);
-    auto fits = [&](size_t vb) {
-        const size_t sm = std::max(fm::lanes_smem_bytes(f, vb), fm::lanes_smem_bytes(b, vb));
-        return sm <= kMaxSmem && fm::lanes_max_active(vb, f) >= 1 && fm::lanes_max_active(vb, b) >= 1;
-    };
-    const bool ok32 = fits(4), ok64 = fits(8);
-    if (!ok32 && !ok64) return FM_OK;
-    auto group_first = [](const fm::ClusterPlan& p) {
-        std::vector<uint32_t> gf(p.n_groups + 1, 0);
-        for (uint32_t l = 0; l < p.n_levels; ++l)
-            for (uint32_t g = p.lvl_gptr[l]; g < p.lvl_gptr[l + 1]; ++g)
-                gf[g] = p.lvl_ptr[l] + 32 * (g - p.lvl_gptr[l]);
-        gf[p.n_groups] = p.n_levels ? p.lvl_ptr[p.n_levels] : 0;
-        return gf;
-    };
-    const std::vector<uint32_t> gff = group_first(pf), gfb = group_first(pb);
-    CK(upload(c->cl_lvl_f, pf.lvl_gptr.data(), pf.lvl_gptr.size(), c->stream));
-    CK(upload(c->cl_lvl_b, pb.lvl_gptr.data(), pb.lvl_gptr.size(), c->stream));
-    CK(upload(c->cl_rec_f, reinterpret_cast<const uint4*>(pf.rec.data()), pf.rec.size() / 4,
-              c->stream));
-    CK(upload(c->cl_rec_b, reinterpret_cast<const uint4*>(pb.rec.data()), pb.rec.size() / 4,
-              c->stream));
-    CK(upload(c->cl_nslot, nslot.data(), nslot.size(), c->stream));
-    CK(upload(c->cl_rptr_f, pf.reset_ptr.data(), pf.reset_ptr.size(), c->stream));
-    CK(upload(c->cl_rptr_b, pb.reset_ptr.data(), pb.reset_ptr.size(), c->stream));
-    CK(upload(c->cl_reset_f, pf.reset.data(), pf.reset.size(), c->stream));
-    CK(upload(c->cl_reset_b, pb.reset.data(), pb.reset.size(), c->stream));
-    CK(upload(c->cl_card_f, gff.data(), gff.size(), c->stream));
-    CK(upload(c->cl_card_b, gfb.data(), gfb.size(), c->stream));
-    f.lvl_ptr = c->cl_lvl_f.p;
-    f.rec = c->cl_rec_f.p;
-    f.nslot = c->cl_nslot.p;
-    f.reset_ptr = c->cl_rptr_f.p;
-    f.reset = c->cl_reset_f.p;
-    b.lvl_ptr = c->cl_lvl_b.p;
-    b.rec = c->cl_rec_b.p;
-    b.nslot = c->cl_nslot.p;
-    b.reset_ptr = c->cl_rptr_b.p;
-    b.reset = c->cl_reset_b.p;
-    c->cl_f = f;
-    c->cl_b = b;
-    c->cl_ok32 = ok32;
-    c->cl_ok64 = ok64;
-    c->cl_lanes = true;
-    CK(cudaStreamSynchronize(c->stream));
-    return FM_OK;
-}
-
-// Plans for the cluster solves: the largest cluster (16, then 8 CTAs of 32
-// warps) whose plan fits and that the device can make resident.  Selected
-// with FM_TRSV_PATH=cluster in the environment; the grid-wide pipelined
-// solves are the default.
-fm_status setup_cluster_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
-                               const std::vector<uint32_t>& lo, const std::vector<uint32_t>& up,
-                               const std::vector<uint32_t>& uo) {
-    c->cl_ok32 = c->cl_ok64 = false;
-    c->cl_lanes = false;
-    const char* path = getenv("FM_TRSV_PATH");
-    if (!path) return FM_OK;
-    if (std::strcmp(path, "lanes") == 0) return setup_lane_solves(c, lp, lo, up, uo);
-    if (std::strcmp(path, "cluster") != 0) return FM_OK;
-    constexpr uint32_t kWarps = 32, kMaxSlots = 4096;
-    constexpr size_t kMaxSmem = 227 * 1024;
-    const char* wenv = getenv("FM_TRSV_WINDOW");
-    const uint32_t window = wenv ? std::max(1u, (uint32_t)strtoul(wenv, nullptr, 10)) : 8u;
-    for (uint32_t cs : {16u, 8u}) {
-        fm::ClusterPlan pf, pb;
-        std::vector<uint32_t> nslot;
-        if (!fm::cluster_plan(c->graph, true, lp, lo, cs, kWarps, window, kMaxSlots, pf, nslot) ||
-            !fm::cluster_plan(c->graph, false, up, uo, cs, kWarps, window, kMaxSlots, pb, nslot))
-            continue;
-        if (pf.max_per_warp > 32 || pb.max_per_warp > 32) continue;
-        auto view = [](const fm::ClusterPlan& p) {
-            fm::ClusterSolve v;
-            v.n_levels = p.n_levels;
-            v.n_ctas = p.n_ctas;
-            v.warps_per_cta = p.warps_per_cta;
-            v.max_per_warp = std::max(p.max_per_warp, 1u);
-            v.maxc = std::max(p.max_cnt, 1u);
-            v.pool_slots = std::max(p.slots_per_cta, 1u);
-            v.window = p.window;
-            return v;
-        };
-        fm::ClusterSolve f = view(pf), b = view(pb);
-        auto fits = [&](size_t vb) {
-            const int st = fm::cluster_stages(vb);
-            const size_t sm = std::max(fm::cluster_smem_bytes(f, vb, st),
-                                       fm::cluster_smem_bytes(b, vb, st));
-            return sm <= kMaxSmem && fm::cluster_max_active(vb, (int)cs, sm) >= 1;
-        };
-        const bool ok32 = fits(4), ok64 = fits(8);
-        if (!ok32 && !ok64) continue;
-        CK(upload(c->cl_lvl_f, pf.lvl_ptr.data(), pf.lvl_ptr.size(), c->stream));
-        CK(upload(c->cl_lvl_b, pb.lvl_ptr.data(), pb.lvl_ptr.size(), c->stream));
-        CK(upload(c->cl_rec_f, reinterpret_cast<const uint4*>(pf.rec.data()), pf.rec.size() / 4,
-                  c->stream));
-        CK(upload(c->cl_rec_b, reinterpret_cast<const uint4*>(pb.rec.data()), pb.rec.size() / 4,
-                  c->stream));
-        CK(upload(c->cl_nslot, nslot.data(), nslot.size(), c->stream));
-        CK(upload(c->cl_rptr_f, pf.reset_ptr.data(), pf.reset_ptr.size(), c->stream));
-        CK(upload(c->cl_rptr_b, pb.reset_ptr.data(), pb.reset_ptr.size(), c->stream));
-        CK(upload(c->cl_reset_f, pf.reset.data(), pf.reset.size(), c->stream));
-        CK(upload(c->cl_reset_b, pb.reset.data(), pb.reset.size(), c->stream));
-        std::vector<uint32_t> card;
-        fm::cluster_card_index(pf.lvl_ptr, cs * kWarps, card);
-        CK(upload(c->cl_card_f, card.data(), card.size(), c->stream));
-        fm::cluster_card_index(pb.lvl_ptr, cs * kWarps, card);
-        CK(upload(c->cl_card_b, card.data(), card.size(), c->stream));
-        f.lvl_ptr = c->cl_lvl_f.p;
-        f.rec = c->cl_rec_f.p;
-        f.nslot = c->cl_nslot.p;
-        f.reset_ptr = c->cl_rptr_f.p;
-        f.reset = c->cl_reset_f.p;
-        b.lvl_ptr = c->cl_lvl_b.p;
-        b.rec = c->cl_rec_b.p;
-        b.nslot = c->cl_nslot.p;
-        b.reset_ptr = c->cl_rptr_b.p;
-        b.reset = c->cl_reset_b.p;
-        c->cl_f = f;
-        c->cl_b = b;
-        c->cl_ok32 = ok32;
-        c->cl_ok64 = ok64;
-        CK(cudaStreamSynchronize(c->stream));
-        return FM_OK;
-    }
-    return FM_OK;
-}
-
-// z = U^-1 L^-1 r on the node-block factors (tmp: the intermediate); the
-// cluster-synchronous solves where the context has them, else the
-// grid-wide pipelined ones.  Returns the kernels launched.
-template <typename T>
-DevBuf<unsigned char>& packed_cards(fm_ctx* c, bool fwd);
-
+// z = U^-1 L^-1 r on the node-block factors (tmp: the intermediate): the
+// slab-partitioned push solves where the context has a plan for this value
+// width, else the grid-wide pipelined ones.  Returns the kernels launched.
 template <typename T>
 int precond_nodes(fm_ctx* c, const T* lu, const T* dinv, const T* r, T* tmp, T* z,
                   unsigned* status) {
@@ -653,21 +498,6 @@ int precond_nodes(fm_ctx* c, const T* lu, const T* dinv, const T* r, T* tmp, T* 
         // a launch the device refuses: the pipelined solves from now on
         cudaGetLastError();
         c->pu_ok32 = c->pu_ok64 = false;
-    }
-    const bool cl = sizeof(T) == 4 ? c->cl_ok32 : c->cl_ok64;
-    if (cl && c->nn) {
-        const cudaError_t e =
-            c->cl_lanes
-                ? fm::launch_trsv_lanes<T>(c->cl_f, c->cl_b, c->cl_card_f.p, c->cl_card_b.p,
-                                           packed_cards<T>(c, true).p, packed_cards<T>(c, false).p,
-                                           r, tmp, z, status, c->stream)
-                : fm::launch_trsv_cluster<T>(c->cl_f, c->cl_b, packed_cards<T>(c, true).p,
-                                             packed_cards<T>(c, false).p, r, tmp, z, status,
-                                             c->stream);
-        if (e == cudaSuccess) return 2;
-        // a launch the device refuses: the pipelined solves from now on
-        cudaGetLastError();
-        c->cl_ok32 = c->cl_ok64 = false;
     }
     fm::launch_trsv_nodes<T>(node_sched(c), lu, dinv, r, tmp, z, status, c->device, c->stream);
     return 4;
@@ -697,8 +527,7 @@ struct Op {
     }
     void precond(const T* r, T* z) const {
         const bool pu = node_block && (sizeof(T) == 4 ? c->pu_ok32 : c->pu_ok64);
-        const bool cl = node_block && (sizeof(T) == 4 ? c->cl_ok32 : c->cl_ok64);
-        PROF(FM_PROF_TRSV, pu ? (r != z ? 3 : 4) : node_block && !cl ? 4 : 2);
+        PROF(FM_PROF_TRSV, pu ? (r != z ? 3 : 4) : node_block ? 4 : 2);
         if (node_block) {
             precond_nodes<T>(c, LU, dinv, r, tmp, z, c->status());
             return;
@@ -754,36 +583,12 @@ fm_status pcg_core(fm_ctx* c, const Op<T>& A, uint32_t n, const T* b, T* x, doub
 }
 
 template <typename T>
-DevBuf<unsigned char>& packed_cards(fm_ctx* c, bool fwd) {
-    if (sizeof(T) == 4) return fwd ? c->cl_pack32_f : c->cl_pack32_b;
-    return fwd ? c->cl_pack64_f : c->cl_pack64_b;
-}
-
-template <typename T>
 fm_status ilu_core(fm_ctx* c, SolverCsr& S, const T* a, T* lu, T* diag) {
-    const bool cl = &S == &c->fem && (sizeof(T) == 4 ? c->cl_ok32 : c->cl_ok64);
-    PROF(FM_PROF_ILU, cl ? 3 : 1);
+    PROF(FM_PROF_ILU, 1);
     if (&S == &c->fem) {
         fm::launch_ilu0_nodes<T>(node_sched(c), a, lu, diag, work<T>(c).dinv.p, c->done.p,
                                  next_epoch(c), c->status(), c->device, c->stream);
         CK(cudaGetLastError());
-        if (cl) {
-            // the cluster solves read the factors as packed cards
-            DevBuf<unsigned char>& pf = packed_cards<T>(c, true);
-            DevBuf<unsigned char>& pb = packed_cards<T>(c, false);
-            if (c->cl_lanes) {
-                CK(pf.reserve((size_t)c->cl_f.n_groups * fm::lanes_card_bytes(c->cl_f, sizeof(T))));
-                CK(pb.reserve((size_t)c->cl_b.n_groups * fm::lanes_card_bytes(c->cl_b, sizeof(T))));
-                fm::launch_pack_groups<T>(c->cl_f, c->cl_b, c->cl_card_f.p, c->cl_card_b.p, lu,
-                                          work<T>(c).dinv.p, pf.p, pb.p, c->stream);
-            } else {
-                CK(pf.reserve((size_t)c->nn * fm::cluster_card_bytes(c->cl_f, sizeof(T))));
-                CK(pb.reserve((size_t)c->nn * fm::cluster_card_bytes(c->cl_b, sizeof(T))));
-                fm::launch_pack_cards<T>(c->cl_f, c->cl_b, c->cl_card_f.p, c->cl_card_b.p, c->nn,
-                                         lu, work<T>(c).dinv.p, pf.p, pb.p, c->stream);
-            }
-            CK(cudaGetLastError());
-        }
         return FM_OK;
     }
     const fm::CsrDev v = S.view();
@@ -892,6 +697,26 @@ fm_status fm_clear_flags(fm_ctx* c) {
     return FM_OK;
 }
 
+fm_status fm_set_wait_limit(fm_ctx* c, uint64_t cycles) {
+    if (!c) return FM_ERR_ARG;
+    const uint64_t units = (cycles + 1023) >> 10;
+    if (units > 0xffffffffull) return fail(c, FM_ERR_ARG, "wait limit too large");
+    c->h_sc->wait_budget = (unsigned)units;
+    CK(cudaMemcpyAsync(&c->sc.p->wait_budget, &c->h_sc->wait_budget, sizeof(unsigned),
+                       cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return FM_OK;
+}
+
+fm_status fm_check_wait(fm_ctx* c) {
+    if (!c) return FM_ERR_ARG;
+    fm::launch_wait_probe(&c->sc.p->never, c->status(), c->stream);
+    CK(cudaGetLastError());
+    uint32_t flags;
+    TRY(device_flags(c, &flags));
+    return check_flags(c, flags, "fm_check_wait");
+}
+
 fm_status fm_sizes(const fm_ctx* c, uint32_t* n_nodes, uint32_t* n_elems, uint32_t* n_dofs,
                    uint64_t* nnz) {
     if (!c) return FM_ERR_ARG;
@@ -984,7 +809,6 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
             const std::vector<uint4> rb = node_records(c->graph, uo);
             CK(upload(c->node_fwd_rec, rf.data(), rf.size(), c->stream));
             CK(upload(c->node_bwd_rec, rb.data(), rb.size(), c->stream));
-            TRY(setup_cluster_solves(c, lp, lo, up, uo));
             TRY(setup_push_solves(c, lp, lo, up, uo));
             CK(cudaStreamSynchronize(c->stream));
             CK(c->done.reserve(std::max<size_t>(c->done.n, (size_t)c->nn + 1)));
@@ -1263,16 +1087,17 @@ fm_status fm_ilu0_apply(fm_ctx* c, const double* r, double* y) {
 struct NoAllocScratch {
     double z[FM_NOALLOC_MAX_DOFS];
     unsigned status;
+    unsigned wait_budget;  // the calling context's wait limit (read after status)
 };
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
 constexpr int kNoAllocMaxDevices = 64;
 
 // Device address of g_noalloc_scratch, looked up once per device with that
-// device current.  The lookup may load the module, so the first call on a
-// device belongs before any stream capture.  (Host code must never pass
-// g_noalloc_scratch itself to a kernel: on the host that name is a stand-in,
-// not a device address.)
+// device current (the caller's current device is restored afterwards).  The
+// lookup may load the module.  (Host code must never pass g_noalloc_scratch
+// itself to a kernel: on the host that name is a stand-in, not a device
+// address.)
 static fm_status noalloc_scratch(fm_ctx* c, NoAllocScratch** out) {
     static std::mutex mu;
     static NoAllocScratch* addr[kNoAllocMaxDevices] = {};
@@ -1281,9 +1106,13 @@ static fm_status noalloc_scratch(fm_ctx* c, NoAllocScratch** out) {
                     kNoAllocMaxDevices);
     std::lock_guard<std::mutex> lock(mu);
     if (!addr[c->device]) {
+        int prev = 0;
+        CK(cudaGetDevice(&prev));
         CK(cudaSetDevice(c->device));
         NoAllocScratch* ptr = nullptr;
-        CK(cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch));
+        const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
+        CK(cudaSetDevice(prev));
+        CK(e);
         addr[c->device] = ptr;
     }
     *out = addr[c->device];
@@ -1301,8 +1130,11 @@ fm_status fm_ilu0_apply_noalloc(fm_ctx* c, const double* r, double* y) {
     NoAllocScratch* sp = nullptr;
     TRY(noalloc_scratch(c, &sp));
     // the status word keeps the previous call's bits: it must start at zero;
-    // z is refilled with the wait sentinel by the launcher before each solve
+    // the wait limit is this context's; z is refilled with the wait sentinel
+    // by the launcher before each solve
     CK(cudaMemsetAsync(&sp->status, 0, sizeof(unsigned), c->stream));
+    CK(cudaMemcpyAsync(&sp->wait_budget, &c->sc.p->wait_budget, sizeof(unsigned),
+                       cudaMemcpyDeviceToDevice, c->stream));
     precond_nodes<double>(c, c->w64.LU.p, c->w64.dinv.p, r, sp->z, y, &sp->status);
     CK(cudaGetLastError());
     unsigned flags = 0;
@@ -1399,12 +1231,32 @@ fm_status fm_csr_pcg_ilu0(fm_ctx* c, uint32_t n, const uint32_t* row_ptr,
     return FM_OK;
 }
 
-fm_status fm_newton_step(fm_ctx* c, double* u, double load_frac, double rtol, double atol,
-                         double inner_tol, int max_newton, int max_pcg, int line_search,
-                         double ls_c, fm_precision prec, int* newton_iters, int* pcg_iters,
-                         double* final_relres) {
+fm_status fm_newton_config_default(fm_newton_config* g) {
+    if (!g) return FM_ERR_ARG;
+    g->newton_rtol = 1e-10;
+    g->newton_atol = 0.0;
+    g->inner_tol = 1e-12;
+    g->predictor_tol = 0.0;
+    g->inner_tol_min = 0.0;
+    g->max_newton = 200;
+    g->max_pcg = 5000;
+    g->line_search = 10;
+    g->ls_c = 1e-4;
+    g->diverge_rate = 0.0;
+    g->diverge_count = 3;
+    g->diverge_growth = 10.0;
+    g->precision = FM_FP64;
+    return FM_OK;
+}
+
+fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_newton_config* g,
+                             fm_newton_result* res) {
+    if (res) std::memset(res, 0, sizeof *res);
     TRY(need_material(c));
-    if (!u || max_newton < 1 || line_search < 0) return fail(c, FM_ERR_ARG, "bad argument");
+    if (!u || !g || g->max_newton < 1 || g->line_search < 0 || g->max_pcg < 1 ||
+        !(g->inner_tol > 0.0))
+        return fail(c, FM_ERR_ARG, "bad argument");
+    const int prec = g->precision;
     if (prec != FM_FP64 && prec != FM_MIXED) return fail(c, FM_ERR_ARG, "unknown precision");
     const bool mixed = prec == FM_MIXED;
     if (mixed) TRY(ensure_matrix<float>(c));
@@ -1414,33 +1266,55 @@ fm_status fm_newton_step(fm_ctx* c, double* u, double load_frac, double rtol, do
     const fm::MeshDev m = mesh_view(c);
     double* R = c->vec_a.p;
     double* du = c->vec_b.p;
-    int n_newton = 0, n_pcg = 0;
-    double r0 = 0.0, last_rel = 0.0;
-    bool have_r0 = false, conv = false;
+    const bool keep_du = g->line_search > 0;
+    int n_newton = 0, n_pcg = 0, n_bt = 0, slow = 0;
+    double r0 = 0.0, rn = 0.0, r_prev = 0.0;
+    double tol = g->inner_tol;
+    bool have_r0 = false;
+    fm_status out = FM_OK;
+    c->newton_hist.clear();
+    auto record = [&](int kind, int its, double rnorm, double alpha, double itol) {
+        if (c->newton_hist.size() < 4096)
+            c->newton_hist.push_back({kind, its, rnorm, alpha, itol, c->h_sc->status, 0u});
+    };
 
-    // ILU(0) of the eliminated tangent, PCG on R (norm rn), then either
-    // u += du (no line search) or du kept in `du` (FP64) for the caller.
-    auto solve = [&](double rn, bool keep_du, int* its) -> fm_status {
+    // ILU(0) of the eliminated tangent, PCG on R (norm rnorm) to itol, then
+    // either u += du or du kept in `du` (FP64) for the line search.
+    auto solve = [&](double rnorm, double itol, bool keep, int* its) -> fm_status {
         if (mixed) {
             // FP32 tangent/ILU(0)/PCG on R/||R||; the step is rescaled in FP64
             TRY(ilu_core<float>(c, c->fem, c->w32.K.p, c->w32.LU.p, c->w32.diag.p));
-            { PROF(FM_PROF_VECTOR, 1); fm::launch_to_f32_scaled(c->n, R, 1.0 / rn, c->w32.b.p, c->w32.x.p, c->stream); }
+            { PROF(FM_PROF_VECTOR, 1); fm::launch_to_f32_scaled(c->n, R, 1.0 / rnorm, c->w32.b.p, c->w32.x.p, c->stream); }
             Op<float> A{c, &c->fem, true, c->w32.K.p, c->w32.LU.p, c->w32.diag.p, c->w32.t.p,
                         c->grid_trsv32, c->w32.dinv.p};
-            TRY(pcg_core<float>(c, A, c->n, c->w32.b.p, c->w32.x.p, inner_tol, max_pcg, its,
+            TRY(pcg_core<float>(c, A, c->n, c->w32.b.p, c->w32.x.p, itol, g->max_pcg, its,
                                 nullptr));
-            if (keep_du) { PROF(FM_PROF_VECTOR, 1); fm::launch_f32_to_f64_scaled(c->n, c->w32.x.p, rn, du, c->stream); }
-            else { PROF(FM_PROF_VECTOR, 1); fm::launch_axpy_u_f32(c->n, c->w32.x.p, rn, u, c->stream); }
+            if (keep) { PROF(FM_PROF_VECTOR, 1); fm::launch_f32_to_f64_scaled(c->n, c->w32.x.p, rnorm, du, c->stream); }
+            else { PROF(FM_PROF_VECTOR, 1); fm::launch_axpy_u_f32(c->n, c->w32.x.p, rnorm, u, c->stream); }
         } else {
             TRY(ilu_core<double>(c, c->fem, c->w64.K.p, c->w64.LU.p, c->w64.diag.p));
             CK(cudaMemsetAsync(du, 0, sizeof(double) * c->n, c->stream));
             Op<double> A{c, &c->fem, true, c->w64.K.p, c->w64.LU.p, c->w64.diag.p, c->w64.t.p,
                          c->grid_trsv64, c->w64.dinv.p};
-            TRY(pcg_core<double>(c, A, c->n, R, du, inner_tol, max_pcg, its, nullptr));
-            if (!keep_du) { PROF(FM_PROF_VECTOR, 1); fm::launch_axpy_u(c->n, du, u, c->stream); }
+            TRY(pcg_core<double>(c, A, c->n, R, du, itol, g->max_pcg, its, nullptr));
+            if (!keep) { PROF(FM_PROF_VECTOR, 1); fm::launch_axpy_u(c->n, du, u, c->stream); }
         }
         CK(cudaGetLastError());
         return FM_OK;
+    };
+
+    auto finish = [&](fm_status st) -> fm_status {
+        c->w64.factor_valid = c->w32.factor_valid = false;
+        if (res) {
+            res->newton_iters = n_newton;
+            res->pcg_iters = n_pcg;
+            res->backtracks = n_bt;
+            res->flags = c->h_sc->status;
+            res->rnorm0 = r0;
+            res->rnorm = rn;
+            res->final_relres = r0 > 0 ? rn / r0 : 0.0;
+        }
+        return st;
     };
 
     if (c->has_bc) {
@@ -1451,7 +1325,7 @@ fm_status fm_newton_step(fm_ctx* c, double* u, double load_frac, double rtol, do
                                 u, v, mixed ? c->w32.b.p : nullptr, c->partials.p, c->counter(),
                                 &c->sc.p->norm2, c->stream); }
         TRY(sync_scalars(c));
-        if (c->h_sc->norm2 > 0.0 && max_newton > 0) {
+        if (c->h_sc->norm2 > 0.0) {
             double* f = c->vec_c.p;
             if (mixed) {
                 { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble(m, u, c->w32.K.p, f, nullptr, 0, c->status(), c->stream); }
@@ -1471,64 +1345,163 @@ fm_status fm_newton_step(fm_ctx* c, double* u, double load_frac, double rtol, do
             }
             { PROF(FM_PROF_VECTOR, 1); fm::launch_norm2(c->n, R, c->partials.p, c->counter(), &c->sc.p->norm2, c->stream); }
             TRY(sync_scalars(c));
-            TRY(check_flags(c, c->h_sc->status, "newton predictor"));
-            r0 = std::sqrt(c->h_sc->norm2);
+            if (fm_status st = check_flags(c, c->h_sc->status, "newton predictor")) return finish(st);
+            r0 = rn = std::sqrt(c->h_sc->norm2);
             have_r0 = true;
             int its = 0;
-            if (r0 > 0.0) TRY(solve(r0, false, &its));
+            const double ptol = g->predictor_tol > 0.0 ? g->predictor_tol : tol;
+            if (r0 > 0.0) TRY(solve(r0, ptol, false, &its));
             n_pcg += its;
             ++n_newton;
+            record(0, its, r0, 1.0, ptol);
+            r_prev = r0;
         }
         { PROF(FM_PROF_VECTOR, 1); fm::launch_set_bc_values(c->n, c->mask.p, c->has_bcval ? c->bcval.p : nullptr, load_frac,
                                  u, c->stream); }
     }
 
-    for (int it = n_newton; it < max_newton; ++it) {
+    bool conv = false;
+    for (int it = n_newton; it < g->max_newton; ++it) {
         if (mixed)
             { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble(m, u, c->w32.K.p, nullptr, R, 1, c->status(), c->stream); }
         else
             { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble(m, u, c->w64.K.p, nullptr, R, 1, c->status(), c->stream); }
         { PROF(FM_PROF_VECTOR, 1); fm::launch_norm2(c->n, R, c->partials.p, c->counter(), &c->sc.p->norm2, c->stream); }
         TRY(sync_scalars(c));
-        TRY(check_flags(c, c->h_sc->status, "newton assembly"));
-        const double rn = std::sqrt(c->h_sc->norm2);
+        rn = std::sqrt(c->h_sc->norm2);
+        if (fm_status st = check_flags(c, c->h_sc->status, "newton assembly")) {
+            record(1, 0, rn, 0.0, tol);
+            return finish(fail(c, st, "%s; Newton iteration %d of load %.6g, ||R|| history "
+                                      "(last): %.3e",
+                               c->err.c_str(), it, load_frac, r_prev));
+        }
         if (!have_r0) {
             r0 = rn;
             have_r0 = true;
         }
-        last_rel = r0 > 0 ? rn / r0 : 0.0;
-        if (rn == 0.0 || rn < rtol * r0 || rn < atol) {
+        if (rn == 0.0 || rn < g->newton_rtol * r0 || rn < g->newton_atol) {
             conv = true;
+            record(1, 0, rn, 0.0, tol);
             break;
         }
+        // the reference's divergence test (FEM/adaptive_fem_engine.hpp:2561-2572)
+        if (it > 2) {
+            const double rate = rn / std::max(r_prev, 1e-30);
+            if (g->diverge_rate > 0.0 && rate > g->diverge_rate) ++slow;
+            if ((g->diverge_rate > 0.0 && slow > g->diverge_count) ||
+                (g->diverge_growth > 0.0 && rn > r_prev * g->diverge_growth)) {
+                record(1, 0, rn, 0.0, tol);
+                return finish(fail(c, FM_ERR_DIVERGED,
+                                   "Newton diverging at iteration %d of load %.6g: ||R|| %.3e "
+                                   "(previous %.3e, ||R_0|| %.3e, slow iterations %d; flags: %s)",
+                                   it, load_frac, rn, r_prev, r0, slow,
+                                   flags_text(c->h_sc->status).c_str()));
+            }
+        }
+        // adaptive inner tolerance: an iteration that did not contract by
+        // diverge_rate (0.9 when the rate test is off) tightens the next solves
+        if (g->inner_tol_min > 0.0 && r_prev > 0.0 &&
+            rn > (g->diverge_rate > 0.0 ? g->diverge_rate : 0.9) * r_prev)
+            tol = std::max(g->inner_tol_min, 0.1 * tol);
         int its = 0;
-        TRY(solve(rn, line_search > 0, &its));
-        if (line_search) {
-            // Armijo backtracking on the residual norm with residual-only
-            // re-assembly at each trial point
-            double alpha = 1.0;
-            for (int bt = 0; bt < line_search; ++bt) {
+        TRY(solve(rn, tol, keep_du, &its));
+        double alpha = 1.0;
+        if (keep_du) {
+            // Armijo backtracking on ||R|| with residual-only re-assembly at
+            // each trial point (armijo_line_search_true, :933-985)
+            // flags raised at rejected trial points (a clamped or non-finite
+            // trial) are dropped: the accepted state's next assembly decides
+            const unsigned status0 = c->h_sc->status;
+            for (int bt = 0; bt < g->line_search; ++bt) {
                 { PROF(FM_PROF_VECTOR, 1); fm::launch_trial(c->n, u, alpha, du, c->vec_c.p, c->stream); }
                 { PROF(FM_PROF_ASSEMBLE, 1); fm::launch_assemble(m, c->vec_c.p, static_cast<double*>(nullptr), nullptr, R, 0,
                                     c->status(), c->stream); }
                 { PROF(FM_PROF_VECTOR, 1); fm::launch_norm2(c->n, R, c->partials.p, c->counter(), &c->sc.p->norm2,
                                  c->stream); }
                 TRY(sync_scalars(c));
-                if (std::sqrt(c->h_sc->norm2) <= (1.0 - ls_c * alpha) * rn) break;
-                if (bt + 1 < line_search) alpha *= 0.5;
+                const double rt = std::sqrt(c->h_sc->norm2);
+                if (rt <= (1.0 - g->ls_c * alpha) * rn + 1e-14) break;
+                alpha *= 0.5;
+                ++n_bt;
             }
             { PROF(FM_PROF_VECTOR, 1); fm::launch_trial(c->n, u, alpha, du, u, c->stream); }
+            c->h_sc->status = status0;
+            CK(cudaMemcpyAsync(&c->sc.p->status, &c->h_sc->status, sizeof(unsigned),
+                               cudaMemcpyHostToDevice, c->stream));
+            TRY(sync_scalars(c));
         }
         CK(cudaGetLastError());
         n_pcg += its;
         ++n_newton;
+        record(1, its, rn, alpha, tol);
+        r_prev = rn;
     }
-    c->w64.factor_valid = c->w32.factor_valid = false;
     CK(cudaStreamSynchronize(c->stream));
-    if (newton_iters) *newton_iters = n_newton;
-    if (pcg_iters) *pcg_iters = n_pcg;
-    if (final_relres) *final_relres = last_rel;
-    if (!conv) return fail(c, FM_ERR_NOT_CONVERGED, "Newton hit max_newton=%d", max_newton);
+    if (!conv) {
+        TRY(sync_scalars(c));
+        return finish(fail(c, FM_ERR_NOT_CONVERGED,
+                           "Newton hit max_newton=%d at load %.6g (||R||/||R_0|| = %.3e; flags: %s)",
+                           g->max_newton, load_frac, r0 > 0 ? rn / r0 : 0.0,
+                           flags_text(c->h_sc->status).c_str()));
+    }
+    return finish(out);
+}
+
+fm_status fm_newton_history(const fm_ctx* c, fm_newton_record* out, int cap, int* count) {
+    if (!c || !count || cap < 0 || (cap > 0 && !out)) return FM_ERR_ARG;
+    const int n = (int)std::min<size_t>(c->newton_hist.size(), (size_t)cap);
+    for (int i = 0; i < n; ++i) out[i] = c->newton_hist[i];
+    *count = (int)c->newton_hist.size();
+    return FM_OK;
+}
+
+fm_status fm_newton_step(fm_ctx* c, double* u, double load_frac, double rtol, double atol,
+                         double inner_tol, int max_newton, int max_pcg, int line_search,
+                         double ls_c, fm_precision prec, int* newton_iters, int* pcg_iters,
+                         double* final_relres) {
+    fm_newton_config g;
+    fm_newton_config_default(&g);
+    g.newton_rtol = rtol;
+    g.newton_atol = atol;
+    g.inner_tol = inner_tol;
+    g.max_newton = max_newton;
+    g.max_pcg = max_pcg;
+    g.line_search = line_search;
+    g.ls_c = ls_c;
+    g.precision = prec;
+    fm_newton_result r;
+    const fm_status st = fm_newton_step_cfg(c, u, load_frac, &g, &r);
+    if (newton_iters) *newton_iters = r.newton_iters;
+    if (pcg_iters) *pcg_iters = r.pcg_iters;
+    if (final_relres) *final_relres = r.final_relres;
+    return st;
+}
+
+fm_status fm_newton_solve_cfg(fm_ctx* c, double* u, int first_step, int n_steps,
+                              const fm_newton_config* cfg, fm_newton_result* result) {
+    if (result) std::memset(result, 0, sizeof *result);
+    TRY(need_material(c));
+    if (!u || !cfg || n_steps < 1 || first_step < 1 || first_step > n_steps)
+        return fail(c, FM_ERR_ARG, "bad load-step range");
+    fm_newton_result tot;
+    std::memset(&tot, 0, sizeof tot);
+    fm_status worst = FM_OK;
+    for (int s = first_step; s <= n_steps; ++s) {
+        fm_newton_result r;
+        const fm_status st = fm_newton_step_cfg(c, u, (double)s / (double)n_steps, cfg, &r);
+        tot.newton_iters += r.newton_iters;
+        tot.pcg_iters += r.pcg_iters;
+        tot.backtracks += r.backtracks;
+        tot.flags = r.flags;
+        tot.rnorm0 = r.rnorm0;
+        tot.rnorm = r.rnorm;
+        tot.final_relres = r.final_relres;
+        if (result) *result = tot;
+        if (st == FM_ERR_NOT_CONVERGED) worst = st;
+        else if (st != FM_OK) return st;
+    }
+    if (worst != FM_OK)
+        return fail(c, worst, "a load step hit max_newton=%d", cfg->max_newton);
     return FM_OK;
 }
 
@@ -1536,26 +1509,20 @@ fm_status fm_newton_solve(fm_ctx* c, double* u, int first_step, int n_steps, dou
                           double atol, double inner_tol, int max_newton, int max_pcg,
                           fm_precision prec, int* newton_iters, int* pcg_iters,
                           double* final_relres) {
-    TRY(need_material(c));
-    if (!u || n_steps < 1 || first_step < 1 || first_step > n_steps)
-        return fail(c, FM_ERR_ARG, "bad load-step range");
-    int tn = 0, tp = 0;
-    double rel = 0.0;
-    fm_status worst = FM_OK;
-    for (int s = first_step; s <= n_steps; ++s) {
-        int nn = 0, np = 0;
-        fm_status st = fm_newton_step(c, u, (double)s / (double)n_steps, rtol, atol, inner_tol,
-                                      max_newton, max_pcg, 0, 0.0, prec, &nn, &np, &rel);
-        tn += nn;
-        tp += np;
-        if (st == FM_ERR_NOT_CONVERGED) worst = st;
-        else if (st != FM_OK) return st;
-    }
-    if (newton_iters) *newton_iters = tn;
-    if (pcg_iters) *pcg_iters = tp;
-    if (final_relres) *final_relres = rel;
-    if (worst != FM_OK) return fail(c, worst, "a load step hit max_newton=%d", max_newton);
-    return FM_OK;
+    fm_newton_config g;
+    fm_newton_config_default(&g);
+    g.newton_rtol = rtol;
+    g.newton_atol = atol;
+    g.inner_tol = inner_tol;
+    g.max_newton = max_newton;
+    g.max_pcg = max_pcg;
+    g.precision = prec;
+    fm_newton_result r;
+    const fm_status st = fm_newton_solve_cfg(c, u, first_step, n_steps, &g, &r);
+    if (newton_iters) *newton_iters = r.newton_iters;
+    if (pcg_iters) *pcg_iters = r.pcg_iters;
+    if (final_relres) *final_relres = r.final_relres;
+    return st;
 }
 
 fm_status fm_csr_ilu0(fm_ctx* c, uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx,
@@ -1615,6 +1582,21 @@ fm_status fm_newton_step_host(fm_ctx* c, double* u_host, double load_frac, doubl
     fm_status st = fm_newton_step(c, c->vec_e.p, load_frac, rtol, atol, inner_tol, max_newton,
                                   max_pcg, line_search, ls_c, prec, newton_iters, pcg_iters,
                                   final_relres);
+    if (st != FM_OK && st != FM_ERR_NOT_CONVERGED) return st;
+    CK(cudaMemcpyAsync(u_host, c->vec_e.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return st;
+}
+
+fm_status fm_newton_step_cfg_host(fm_ctx* c, double* u_host, double load_frac,
+                                  const fm_newton_config* cfg, fm_newton_result* result) {
+    TRY(need_mesh(c));
+    if (!u_host) return fail(c, FM_ERR_ARG, "u is null");
+    CK(c->vec_e.reserve(c->n));
+    CK(cudaMemcpyAsync(c->vec_e.p, u_host, sizeof(double) * c->n, cudaMemcpyHostToDevice,
+                       c->stream));
+    const fm_status st = fm_newton_step_cfg(c, c->vec_e.p, load_frac, cfg, result);
     if (st != FM_OK && st != FM_ERR_NOT_CONVERGED) return st;
     CK(cudaMemcpyAsync(u_host, c->vec_e.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost,
                        c->stream));

@@ -15,6 +15,9 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarp = 32;
 // Bounded device waits: a wait that sees no progress for this many SM clock
 // cycles (about 1 s at B200 clocks) records FM_FLAG_TIMEOUT and returns.
+// A context can set another limit (fm_set_wait_limit): it travels in the
+// word after every status word the library hands to kernels, in units of
+// 1024 cycles (0: this default).
 constexpr long long kWaitCycles = 2000000000ll;
 // Reference constants (FEM/adaptive_fem_engine.hpp:102,141,170,308-309).
 constexpr double kJSafe = 0.01;
@@ -33,7 +36,9 @@ struct DevScalars {
     double scale;    // rhs scaling for the FP32 inner solve
     unsigned stop;   // 1: |pAp| < 1e-60 breakdown
     unsigned status; // FM_FLAG_* bits
+    unsigned wait_budget;  // bounded-wait limit in 1024 cycles (0: kWaitCycles); follows status
     unsigned counter[8];  // last-block counters (one per reduction site)
+    unsigned never;       // a flag no kernel sets (fm_check_wait waits on it)
 };
 
 constexpr int kRedBlocks = 296;  // 2 x 148 SMs: fixed grid => fixed summation order
@@ -64,18 +69,24 @@ __device__ __forceinline__ void raise_flag(unsigned* status, unsigned bits) {
     atomicOr(status, bits);
 }
 
+// The wait limit in SM cycles that travels with a status word (the next word).
+__device__ __forceinline__ long long wait_limit(const unsigned* status) {
+    const unsigned b = ld_volatile_u32(status + 1);
+    return b ? (long long)b << 10 : kWaitCycles;
+}
+
 // Spin until *flag == epoch.  Returns false (and sets FM_FLAG_TIMEOUT) when
 // the wait exceeds kWaitCycles or another thread already timed out, so no
 // wait can run unbounded.
 __device__ __forceinline__ bool wait_flag(const unsigned* flag, unsigned epoch,
                                           unsigned* status) {
     if (ld_acquire(flag) == epoch) return true;
-    const long long t0 = clock64();
+    const long long t0 = clock64(), limit = wait_limit(status);
     for (unsigned it = 1;; ++it) {
         if (ld_acquire(flag) == epoch) return true;
         if ((it & 31u) == 0) {
             if (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) return false;
-            if (clock64() - t0 > kWaitCycles) {
+            if (clock64() - t0 > limit) {
                 raise_flag(status, FM_FLAG_TIMEOUT);
                 return false;
             }
@@ -94,7 +105,7 @@ __device__ __forceinline__ bool wait_flags_warp(const unsigned* flag, bool need,
                                                 unsigned* status, unsigned sleep_ns) {
     bool ok = !need || ld_acquire(flag) == epoch;
     if (__all_sync(kFull, ok)) return true;
-    const long long t0 = clock64();
+    const long long t0 = clock64(), limit = wait_limit(status);
     unsigned ns = 32;
     for (unsigned it = 1;; ++it) {
         if (sleep_ns && it > 16) {
@@ -105,7 +116,7 @@ __device__ __forceinline__ bool wait_flags_warp(const unsigned* flag, bool need,
         if (__all_sync(kFull, ok)) return true;
         if ((it & 31u) == 0 &&
             __any_sync(kFull, (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) ||
-                                  clock64() - t0 > kWaitCycles)) {
+                                  clock64() - t0 > limit)) {
             if ((threadIdx.x & 31) == 0) raise_flag(status, FM_FLAG_TIMEOUT);
             return false;
         }

@@ -861,6 +861,16 @@ void launch_trial(uint32_t n, const double* u, double alpha, const double* du, d
     k_axpby_trial<<<kRedBlocks * 2, kVecThreads, 0, s>>>(n, u, alpha, du, y);
 }
 
+// One warp, one bounded wait on a flag that nothing sets: the wait gives up
+// after the status word's wait limit and raises FM_FLAG_TIMEOUT.
+__global__ void __launch_bounds__(32) k_wait_probe(const unsigned* flag, unsigned* status) {
+    wait_flags_warp(flag, true, 1u, status, 0u);
+}
+
+void launch_wait_probe(const unsigned* flag, unsigned* status, cudaStream_t s) {
+    k_wait_probe<<<1, 32, 0, s>>>(flag, status);
+}
+
 // Load-step predictor: v = frac*val - u on constrained DOFs (0 elsewhere),
 // in FP64 and (optionally) FP32; ||v||^2 through the deterministic reduction.
 __global__ void __launch_bounds__(kVecThreads)

@@ -142,6 +142,9 @@ void launch_apply_bc_nodes(uint32_t nn, const uint32_t* nbr_ptr, const uint32_t*
 // y = scale * x (FP32 -> FP64)
 void launch_f32_to_f64_scaled(uint32_t n, const float* x, double scale, double* y,
                               cudaStream_t s);
+// one warp waits (bounded by the limit that travels with status) for *flag
+// to reach epoch 1; nothing sets it, so the wait times out
+void launch_wait_probe(const unsigned* flag, unsigned* status, cudaStream_t s);
 // y = u + alpha du (line-search trial point)
 void launch_trial(uint32_t n, const double* u, double alpha, const double* du, double* y,
                   cudaStream_t s);

@@ -38,58 +38,6 @@ void launch_ilu0_nodes(const NodeSched& S, const T* a, T* lu, T* d, T* dinv, uns
 template <typename T>
 void launch_fill_sentinel(uint32_t n, T* x, cudaStream_t s);
 
-// One direction of the cluster-synchronous solves (fm_trsv_cluster.cu):
-// the level pointers, per-position records {node, first neighbour entry,
-// deg | sk << 8 | cnt << 16, own slot} and per-neighbour-entry slots
-// (cta << 16 | index) of fm_setup.cpp cluster_plan, on the device.
-struct ClusterSolve {
-    uint32_t n_levels = 0, n_ctas = 0, warps_per_cta = 0;
-    uint32_t max_per_warp = 0;  // nodes of one level per warp, at most (<= 32)
-    uint32_t maxc = 0;          // neighbours on the solve's side, at most (<= 32)
-    uint32_t pool_slots = 0;    // value slots per CTA (16 bytes each in FP32, 32 in FP64)
-    uint32_t window = 1;        // levels between cluster barriers
-    uint32_t n_groups = 0;      // lane-group plans: groups of 32 nodes
-    uint32_t sleep_ns = 0;      // lane-group plans: longest sleep between polls
-    const uint32_t* lvl_ptr = nullptr;
-    const uint4* rec = nullptr;
-    const uint32_t* nslot = nullptr;
-    const uint32_t* reset_ptr = nullptr;  // per (window, CTA): slots to reset after it
-    const uint32_t* reset = nullptr;
-};
-// bytes of one packed card, dynamic shared memory of one CTA, stage depth
-size_t cluster_card_bytes(const ClusterSolve& P, size_t value_bytes);
-size_t cluster_smem_bytes(const ClusterSolve& P, size_t value_bytes, int stages);
-int cluster_stages(size_t value_bytes);
-// clusters of cs CTAs (one per SM, 1024 threads, smem bytes each) that can be
-// resident at once for the solve kernels of this value width (0: none)
-int cluster_max_active(size_t value_bytes, int cs, size_t smem);
-// pack the factors into both directions' cards (after each factorization)
-template <typename T>
-void launch_pack_cards(const ClusterSolve& F, const ClusterSolve& B, const uint32_t* card_f,
-                       const uint32_t* card_b, uint32_t n_pos, const T* lu, const T* dinv,
-                       unsigned char* packed_f, unsigned char* packed_b, cudaStream_t s);
-// One-lane-per-node cluster solves (fm_trsv_lanes.cu): lvl_ptr of the plans
-// holds group ranges, grp_* the first position of every group (n_groups+1).
-int lanes_buffers(size_t value_bytes);
-int lanes_max_neighbours();
-size_t lanes_card_bytes(const ClusterSolve& P, size_t value_bytes);
-size_t lanes_smem_bytes(const ClusterSolve& P, size_t value_bytes);
-int lanes_max_active(size_t value_bytes, const ClusterSolve& P);
-template <typename T>
-void launch_pack_groups(const ClusterSolve& F, const ClusterSolve& B, const uint32_t* grp_f,
-                        const uint32_t* grp_b, const T* lu, const T* dinv, unsigned char* cards_f,
-                        unsigned char* cards_b, cudaStream_t s);
-template <typename T>
-cudaError_t launch_trsv_lanes(const ClusterSolve& F, const ClusterSolve& B, const uint32_t* grp_f,
-                              const uint32_t* grp_b, const unsigned char* cards_f,
-                              const unsigned char* cards_b, const T* r, T* tmp, T* y,
-                              unsigned* status, cudaStream_t s);
-// y = U^-1 L^-1 r through tmp from the packed cards
-template <typename T>
-cudaError_t launch_trsv_cluster(const ClusterSolve& F, const ClusterSolve& B,
-                                const unsigned char* packed_f, const unsigned char* packed_b,
-                                const T* r, T* tmp, T* y, unsigned* status, cudaStream_t s);
-
 // Slab-partitioned push solves (fm_trsv_push.cu) on the plan of
 // fm_setup.cpp push_plan: CTA g of the grid (clusters of `cluster` CTAs)
 // walks positions pos_*[g] .. pos_*[g+1] of rec_* ({node, first neighbour

@@ -159,109 +159,6 @@ uint32_t csr_levels(uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx
     return levels_from_depth(depth, maxd, ptr, rows);
 }
 
-bool cluster_plan(const NodeGraph& g, bool lower, const std::vector<uint32_t>& ptr,
-                  const std::vector<uint32_t>& order, uint32_t n_ctas, uint32_t warps_per_cta,
-                  uint32_t window, uint32_t max_slots_per_cta, ClusterPlan& plan,
-                  std::vector<uint32_t>& nslot, bool lanes) {
-    const uint32_t n = g.n_nodes;
-    const uint32_t nl = ptr.empty() ? 0 : (uint32_t)ptr.size() - 1;
-    const uint32_t W = n_ctas * warps_per_cta;
-    if (window < 1) window = 1;
-    const uint32_t n_win = (nl + window - 1) / window;
-    plan = ClusterPlan{};
-    plan.n_levels = nl;
-    plan.n_ctas = n_ctas;
-    plan.warps_per_cta = warps_per_cta;
-    plan.window = window;
-    plan.lvl_ptr = ptr;
-    plan.rec.assign(4 * (size_t)n, 0);
-    plan.lanes = lanes;
-    plan.lvl_gptr.assign(nl + 1, 0);
-    for (uint32_t l = 0; l < nl; ++l)
-        plan.lvl_gptr[l + 1] = plan.lvl_gptr[l] + (ptr[l + 1] - ptr[l] + 31) / 32;
-    plan.n_groups = plan.lvl_gptr[nl];
-    // warp of position p of level l
-    auto warp_of = [&](uint32_t l, uint32_t p) {
-        const uint32_t i = p - ptr[l];
-        return lanes ? (plan.lvl_gptr[l] + i / 32) % W : i % W;
-    };
-    nslot.resize(g.nbr.size(), 0);
-    std::vector<uint32_t> level(n), pos(n), last(n);
-    for (uint32_t l = 0; l < nl; ++l) {
-        const uint32_t width = ptr[l + 1] - ptr[l];
-        const uint32_t units = lanes ? (width + 31) / 32 : width;
-        plan.max_per_warp = std::max(plan.max_per_warp, (units + W - 1) / W);
-        for (uint32_t p = ptr[l]; p < ptr[l + 1]; ++p) {
-            level[order[p]] = l;
-            pos[order[p]] = p;
-        }
-    }
-    // last level that reads each node's values: its dependants are the
-    // neighbours on the other side
-    for (uint32_t i = 0; i < n; ++i) {
-        uint32_t lu = level[i];
-        uint32_t cnt = 0;
-        for (uint32_t k = g.ptr[i]; k < g.ptr[i + 1]; ++k) {
-            const uint32_t j = g.nbr[k];
-            if (lower ? j > i : j < i) lu = std::max(lu, level[j]);
-            if (lower ? j < i : j > i) ++cnt;
-        }
-        last[i] = lu;
-        plan.max_cnt = std::max(plan.max_cnt, cnt);
-    }
-    if (plan.max_cnt > 32) return false;
-    // interval allocation per CTA pool: a slot last read in window t is
-    // reset after the barrier closing t and reused from window t + 2 on
-    std::vector<std::vector<uint32_t>> free_list(n_ctas);
-    std::vector<uint32_t> used(n_ctas, 0);
-    std::vector<std::vector<uint32_t>> release(n_win + 2);  // (cta << 16) | idx
-    std::vector<std::vector<uint32_t>> resets((size_t)n_win * n_ctas);
-    std::vector<uint32_t> slot(n);
-    for (uint32_t l = 0; l < nl; ++l) {
-        if (l % window == 0) {
-            for (uint32_t s : release[l / window]) free_list[s >> 16].push_back(s & 0xffffu);
-            release[l / window].clear();
-        }
-        for (uint32_t p = ptr[l]; p < ptr[l + 1]; ++p) {
-            const uint32_t gw = warp_of(l, p);
-            const uint32_t cta = gw / warps_per_cta;
-            uint32_t idx;
-            if (!free_list[cta].empty()) {
-                idx = free_list[cta].back();
-                free_list[cta].pop_back();
-            } else {
-                idx = used[cta]++;
-                if (used[cta] > max_slots_per_cta || used[cta] > 0xffffu) return false;
-            }
-            const uint32_t node = order[p];
-            slot[node] = (cta << 16) | idx;
-            const uint32_t t = last[node] / window;
-            release[t + 2].push_back(slot[node]);
-            resets[(size_t)t * n_ctas + cta].push_back(idx);
-        }
-    }
-    for (uint32_t c = 0; c < n_ctas; ++c) plan.slots_per_cta = std::max(plan.slots_per_cta, used[c]);
-    plan.reset_ptr.assign((size_t)n_win * n_ctas + 1, 0);
-    for (size_t i = 0; i < resets.size(); ++i) {
-        plan.reset_ptr[i + 1] = plan.reset_ptr[i] + (uint32_t)resets[i].size();
-        plan.reset.insert(plan.reset.end(), resets[i].begin(), resets[i].end());
-    }
-    for (uint32_t p = 0; p < n; ++p) {
-        const uint32_t node = order[p];
-        const uint32_t deg = g.ptr[node + 1] - g.ptr[node], sk = g.self[node];
-        const uint32_t cnt = lower ? sk : deg - sk - 1;
-        plan.rec[4 * (size_t)p + 0] = node;
-        plan.rec[4 * (size_t)p + 1] = g.ptr[node];
-        plan.rec[4 * (size_t)p + 2] = deg | (sk << 8) | (cnt << 16);
-        plan.rec[4 * (size_t)p + 3] = slot[node] & 0xffffu;
-        for (uint32_t k = g.ptr[node]; k < g.ptr[node + 1]; ++k) {
-            const uint32_t j = g.nbr[k];
-            if (lower ? j < node : j > node) nslot[k] = slot[j];
-        }
-    }
-    return true;
-}
-
 bool push_plan(const NodeGraph& g, const std::vector<uint32_t>& fwd_ptr,
                const std::vector<uint32_t>& fwd_order, const std::vector<uint32_t>& bwd_ptr,
                const std::vector<uint32_t>& bwd_order, uint32_t n_clusters, uint32_t cluster,
@@ -411,17 +308,6 @@ void ilu_edge_maps(const NodeGraph& g, std::vector<uint32_t>& ptr, std::vector<u
                 if (hit != ni + di && *hit == g.nbr[q]) map[o] = (uint8_t)(hit - ni);
             }
         }
-    }
-}
-
-void cluster_card_index(const std::vector<uint32_t>& lvl_ptr, uint32_t W,
-                        std::vector<uint32_t>& card_of_pos) {
-    const uint32_t nl = lvl_ptr.empty() ? 0 : (uint32_t)lvl_ptr.size() - 1;
-    card_of_pos.assign(nl ? lvl_ptr[nl] : 0, 0);
-    for (uint32_t l = 0; l < nl; ++l) {
-        const uint32_t a = lvl_ptr[l], width = lvl_ptr[l + 1] - a;
-        for (uint32_t i = 0; i < width; ++i)
-            card_of_pos[a + i] = first_card(a, width, W, i % W) + i / W;
     }
 }
 

@@ -62,45 +62,6 @@ uint32_t csr_levels(uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx
 uint32_t node_levels(const NodeGraph& g, bool lower, std::vector<uint32_t>& ptr,
                      std::vector<uint32_t>& order);
 
-// Plan of a triangular solve on one thread-block cluster: warp
-// gw = cta * warps_per_cta + w takes positions lvl_ptr[l] + gw, + gw + W, ...
-// of each dependency level (W = all warps).  The three values a node
-// produces live, from its level to the last level that reads them, in a
-// slot of its writer CTA's shared-memory pool.  Levels are grouped in
-// windows of `window` levels closed by a cluster barrier; a slot whose last
-// read falls in window t is reset (to the wait sentinel) by its CTA after
-// the barrier closing window t and handed out again from window t + 2 on.
-struct ClusterPlan {
-    uint32_t n_levels = 0, n_ctas = 0, warps_per_cta = 0, window = 1;
-    uint32_t max_per_warp = 0;   // nodes one warp takes in one level, at most
-    uint32_t max_cnt = 0;        // neighbours on the solve's side of one node, at most
-    uint32_t slots_per_cta = 0;  // pool entries the busiest CTA needs
-    std::vector<uint32_t> lvl_ptr;  // n_levels + 1 positions
-    // per position: {node, first neighbour entry, deg | sk << 8 | cnt << 16, own slot}
-    std::vector<uint32_t> rec;      // 4 words per position
-    // slots CTA c resets after window t: reset[reset_ptr[t * n_ctas + c] ...
-    // reset_ptr[t * n_ctas + c + 1])
-    std::vector<uint32_t> reset_ptr, reset;
-    // lane groups (lanes = true): a level's positions in groups of 32, group
-    // i of level l is global group lvl_gptr[l] + i, taken by warp
-    // (global group) mod W, lane = position within the group
-    bool lanes = false;
-    uint32_t n_groups = 0;
-    std::vector<uint32_t> lvl_gptr;  // n_levels + 1
-};
-
-// Builds the plan of one direction (lower: forward solve over the levels
-// ptr/order of node_levels(g, true, ...)) and writes, for every neighbour
-// entry on that side (lower entries for the forward solve, upper ones for
-// the backward), the neighbour's slot as (cta << 16) | index into nslot
-// (g.nbr.size() entries; the other side's entries are left as they are).
-// Returns false when a CTA pool would need more than max_slots_per_cta
-// entries or a side has more than 32 neighbours.
-bool cluster_plan(const NodeGraph& g, bool lower, const std::vector<uint32_t>& ptr,
-                  const std::vector<uint32_t>& order, uint32_t n_ctas, uint32_t warps_per_cta,
-                  uint32_t window, uint32_t max_slots_per_cta, ClusterPlan& plan,
-                  std::vector<uint32_t>& nslot, bool lanes = false);
-
 // Structural map of the ILU(0) updates (node granularity): for node n and
 // its k-th lower neighbour m (k < self[n]), entry t of
 // map[ptr[n] + sum_{k'<k} (deg(m') - self(m')) + t], t = 0 .. deg(m) - self(m) - 1,
@@ -166,18 +127,5 @@ bool push_plan(const NodeGraph& g, const std::vector<uint32_t>& fwd_ptr,
                const std::vector<uint32_t>& fwd_order, const std::vector<uint32_t>& bwd_ptr,
                const std::vector<uint32_t>& bwd_order, uint32_t n_clusters, uint32_t cluster,
                uint32_t block, uint32_t max_slots, PushPlan& plan);
-
-// Cards of the cluster solves are ordered by (level, warp, node): position
-// level_start + gw + j W of a level of `width` positions is warp gw's j-th
-// node there, and warp gw holds q + (gw < r) of the level's cards
-// (width = q W + r), starting at
-FM_HD inline uint32_t first_card(uint32_t level_start, uint32_t width, uint32_t W,
-                                 uint32_t gw) {
-    const uint32_t q = width / W, r = width % W;
-    return level_start + gw * q + (gw < r ? gw : r);
-}
-// card index of every position of the levels lvl_ptr
-void cluster_card_index(const std::vector<uint32_t>& lvl_ptr, uint32_t W,
-                        std::vector<uint32_t>& card_of_pos);
 
 }  // namespace fm

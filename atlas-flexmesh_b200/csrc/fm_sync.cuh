@@ -62,7 +62,7 @@ __device__ __forceinline__ void wait_values3_warp(const T* p, unsigned* status, 
         need = Sentinel<T>::is(v0) | Sentinel<T>::is(v1) | Sentinel<T>::is(v2);
     }
     if (!__any_sync(kFull, need)) return;
-    const long long t0 = clock64();
+    const long long t0 = clock64(), limit = wait_limit(status);
     unsigned ns = 32;
     for (unsigned it = 1;; ++it) {
         if (sleep_ns && it > 16) {
@@ -78,7 +78,7 @@ __device__ __forceinline__ void wait_values3_warp(const T* p, unsigned* status, 
         if (!__any_sync(kFull, need)) return;
         if ((it & 63u) == 0 &&
             __any_sync(kFull, (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) ||
-                                  clock64() - t0 > kWaitCycles)) {
+                                  clock64() - t0 > limit)) {
             if ((threadIdx.x & 31) == 0) raise_flag(status, FM_FLAG_TIMEOUT);
             return;
         }

@@ -150,7 +150,7 @@ __device__ __forceinline__ void wait_push(uint32_t sl, const T* gp, unsigned* st
         need = poll();
     }
     if (!__any_sync(kFull, need)) return;
-    const long long t0 = clock64();
+    const long long t0 = clock64(), limit = wait_limit(status);
     for (unsigned it = 1;; ++it) {
         if (need) need = poll();
         if (!__any_sync(kFull, need)) return;
@@ -158,7 +158,7 @@ __device__ __forceinline__ void wait_push(uint32_t sl, const T* gp, unsigned* st
         // timeout flag every 256 rounds
         if ((it & 255u) == 0 &&
             __any_sync(kFull, (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) ||
-                                  clock64() - t0 > kWaitCycles)) {
+                                  clock64() - t0 > limit)) {
             if ((threadIdx.x & 31) == 0) raise_flag(status, FM_FLAG_TIMEOUT);
             return;
         }

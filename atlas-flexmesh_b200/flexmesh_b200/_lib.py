@@ -17,7 +17,8 @@ FM_FP64, FM_MIXED = 0, 1
 FM_PATTERN_REFERENCE, FM_PATTERN_SOLVE = 0, 1
 STATUS = {0: "FM_OK", 1: "FM_ERR_ARG", 2: "FM_ERR_CUDA", 3: "FM_ERR_OOM", 4: "FM_ERR_NONFINITE",
           5: "FM_ERR_ZERO_PIVOT", 6: "FM_ERR_INVERTED", 7: "FM_ERR_TIMEOUT",
-          8: "FM_ERR_NOT_CONVERGED", 9: "FM_ERR_LIMITS"}
+          8: "FM_ERR_NOT_CONVERGED", 9: "FM_ERR_LIMITS", 10: "FM_ERR_DIVERGED"}
+FM_ERR_NOT_CONVERGED, FM_ERR_DIVERGED = 8, 10
 FLAG_NONFINITE, FLAG_INVERTED, FLAG_J_CLAMPED, FLAG_PIVOT, FLAG_TIMEOUT, FLAG_BREAKDOWN = (
     1, 2, 4, 8, 16, 32)
 
@@ -29,13 +30,37 @@ EXPORTS = [
     "fm_residual", "fm_assemble_reference_pattern", "fm_levels", "fm_ilu0", "fm_get_ilu0",
     "fm_ilu0_apply", "fm_ilu0_apply_noalloc", "fm_spmv", "fm_pcg", "fm_csr_pcg_ilu0", "fm_newton_solve",
     "fm_exact_apply", "fm_adjoint", "fm_csr_ilu0", "fm_newton_step", "fm_newton_step_host",
-    "fm_profile_enable", "fm_profile_read",
+    "fm_profile_enable", "fm_profile_read", "fm_newton_config_default", "fm_newton_step_cfg",
+    "fm_newton_history", "fm_set_wait_limit", "fm_check_wait", "fm_newton_step_cfg_host",
+    "fm_newton_solve_cfg",
 ]
 PROF_KINDS = {0: "assemble", 1: "ilu0", 2: "trsv", 3: "spmv", 4: "vector"}
 
 
 class Profile(C.Structure):
     _fields_ = [("ms", C.c_double * 8), ("calls", C.c_uint64 * 8), ("kernels", C.c_uint64 * 8)]
+
+
+class NewtonConfig(C.Structure):
+    """fm_newton_config (include/fm_api.h)"""
+    _fields_ = [("newton_rtol", C.c_double), ("newton_atol", C.c_double),
+                ("inner_tol", C.c_double), ("predictor_tol", C.c_double),
+                ("inner_tol_min", C.c_double), ("max_newton", C.c_int), ("max_pcg", C.c_int),
+                ("line_search", C.c_int), ("ls_c", C.c_double), ("diverge_rate", C.c_double),
+                ("diverge_count", C.c_int), ("diverge_growth", C.c_double),
+                ("precision", C.c_int)]
+
+
+class NewtonResult(C.Structure):
+    _fields_ = [("newton_iters", C.c_int), ("pcg_iters", C.c_int), ("backtracks", C.c_int),
+                ("flags", C.c_uint32), ("rnorm0", C.c_double), ("rnorm", C.c_double),
+                ("final_relres", C.c_double)]
+
+
+class NewtonRecord(C.Structure):
+    _fields_ = [("kind", C.c_int), ("pcg_iters", C.c_int), ("rnorm", C.c_double),
+                ("alpha", C.c_double), ("inner_tol", C.c_double), ("flags", C.c_uint32),
+                ("pad", C.c_uint32)]
 
 
 class FMError(RuntimeError):
@@ -91,6 +116,13 @@ def lib() -> C.CDLL:
                                _P(_i32), _P(_i32), _P(_f64)],
             "fm_newton_step_host": [_vp, _vp, _f64, _f64, _f64, _f64, _i32, _i32, _i32, _f64,
                                     _i32, _P(_i32), _P(_i32), _P(_f64)],
+            "fm_newton_config_default": [_P(NewtonConfig)],
+            "fm_newton_step_cfg": [_vp, _vp, _f64, _P(NewtonConfig), _P(NewtonResult)],
+            "fm_newton_history": [_vp, _P(NewtonRecord), _i32, _P(_i32)],
+            "fm_newton_step_cfg_host": [_vp, _vp, _f64, _P(NewtonConfig), _P(NewtonResult)],
+            "fm_newton_solve_cfg": [_vp, _vp, _i32, _i32, _P(NewtonConfig), _P(NewtonResult)],
+            "fm_set_wait_limit": [_vp, _u64],
+            "fm_check_wait": [_vp],
             "fm_profile_enable": [_vp, _i32],
             "fm_profile_read": [_vp, _P(Profile)],
             "fm_exact_apply": [_vp, _vp, _vp, _vp, _i32],
@@ -180,6 +212,14 @@ class Context:
 
     def clear_flags(self):
         self._check(lib().fm_clear_flags(self._h), "fm_clear_flags")
+
+    def set_wait_limit(self, cycles: int = 0):
+        """bounded-wait limit of this context's kernels (SM cycles; 0: default)"""
+        self._check(lib().fm_set_wait_limit(self._h, int(cycles)), "fm_set_wait_limit")
+
+    def check_wait(self):
+        """fm_check_wait: returns its status (FM_ERR_TIMEOUT = 7 expected)"""
+        return lib().fm_check_wait(self._h)
 
     # ------------------------------------------------------------------
     def set_mesh(self, xyz, conn, elem_volume=None):
@@ -367,6 +407,65 @@ class Context:
             self._check(st, "fm_newton_step_host")
         return {"newton_iters": nit.value, "pcg_iters": pit.value, "final_relres": rel.value,
                 "status": st}
+
+    @staticmethod
+    def newton_config(**cfg):
+        """an fm_newton_config: fm_newton_config_default's values with the
+        given fields replaced (prec= is accepted for precision=)"""
+        g = NewtonConfig()
+        lib().fm_newton_config_default(C.byref(g))
+        for k, v in cfg.items():
+            if k == "prec":
+                k = "precision"
+            if k not in {f for f, _ in NewtonConfig._fields_}:
+                raise TypeError(f"unknown Newton option {k}")
+            setattr(g, k, v)
+        return g
+
+    def newton_step_cfg(self, u, load_frac, allow=(), **cfg):
+        """fm_newton_step_cfg: cfg keys are fm_newton_config's fields (the
+        rest keep fm_newton_config_default's values); statuses listed in
+        `allow` are returned in the result instead of raised.  u: a CUDA
+        tensor, or a float64 numpy array (the host-buffer call)"""
+        g = self.newton_config(**cfg)
+        r = NewtonResult()
+        if isinstance(u, np.ndarray):
+            assert u.dtype == np.float64 and u.flags.c_contiguous
+            st = lib().fm_newton_step_cfg_host(self._h, _hp(u), load_frac, C.byref(g),
+                                               C.byref(r))
+        else:
+            st = lib().fm_newton_step_cfg(self._h, _dp(u), load_frac, C.byref(g), C.byref(r))
+        out = {f: getattr(r, f) for f, _ in NewtonResult._fields_}
+        out["status"] = st
+        if st and st not in allow:
+            self._check(st, "fm_newton_step_cfg")
+        if st:
+            buf = C.create_string_buffer(512)
+            lib().fm_last_error(self._h, buf, 512)
+            out["error"] = buf.value.decode(errors="replace")
+        return out
+
+    def newton_solve_cfg(self, u, n_steps, first_step=1, allow=(), **cfg):
+        """fm_newton_solve_cfg over load steps first_step..n_steps"""
+        g = self.newton_config(**cfg)
+        r = NewtonResult()
+        st = lib().fm_newton_solve_cfg(self._h, _dp(u), first_step, n_steps, C.byref(g),
+                                       C.byref(r))
+        out = {f: getattr(r, f) for f, _ in NewtonResult._fields_}
+        out["status"] = st
+        if st and st not in allow:
+            self._check(st, "fm_newton_solve_cfg")
+        return out
+
+    def newton_history(self):
+        """per-solve records of the latest Newton call"""
+        cnt = _i32()
+        lib().fm_newton_history(self._h, None, 0, C.byref(cnt))
+        recs = (NewtonRecord * max(cnt.value, 1))()
+        self._check(lib().fm_newton_history(self._h, recs, cnt.value, C.byref(cnt)),
+                    "fm_newton_history")
+        return [{f: getattr(r, f) for f, _ in NewtonRecord._fields_ if f != "pad"}
+                for r in recs[: cnt.value]]
 
     def profile_enable(self, on=True):
         self._check(lib().fm_profile_enable(self._h, int(on)), "fm_profile_enable")

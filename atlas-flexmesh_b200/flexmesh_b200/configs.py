@@ -119,8 +119,11 @@ def top_face_xy_dofs(xyz):
 
 
 def unit_cube_problem(name, N, *, jitter=0.0, seed_jitter=SEED_JITTER, sigma_log=0.0,
-                      seed_mat=SEED_MAT, nu=0.3, E=1.0, uz_total=-0.1, n_steps=5):
-    xyz, conn = unit_cube(N)
+                      seed_mat=SEED_MAT, nu=0.3, E=1.0, uz_total=-0.1, n_steps=5, mesher=None):
+    """mesher(N) -> (xyz, conn): the unit-cube generator to use (default: the
+    library's fm_unit_cube; a CPU caller that must not load the library
+    passes another generator of the same mesh)"""
+    xyz, conn = (mesher or unit_cube)(N)
     vol = tet_volumes(xyz, conn)
     if jitter:
         xyz = jitter_interior(xyz, N, jitter, seed_jitter)
@@ -137,10 +140,10 @@ def small_block(N=8):
     return unit_cube_problem("small", N, uz_total=-0.1, n_steps=5)
 
 
-def scaleup_block(N=64, n_steps=10):
+def scaleup_block(N=64, n_steps=10, mesher=None):
     """64^3 x 6 tets, interior jitter 0.15 h, log-normal mu (sigma 0.3), u_z=-0.2 in 10 steps"""
     return unit_cube_problem("scaleup", N, jitter=0.15, sigma_log=0.3, uz_total=-0.2,
-                             n_steps=n_steps)
+                             n_steps=n_steps, mesher=mesher)
 
 
 def assembly_block(N=128):

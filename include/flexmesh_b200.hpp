@@ -24,6 +24,8 @@
 #include <stdexcept>
 #include <string>
 #include <tuple>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "fm_api.h"
@@ -221,7 +223,7 @@ struct NewtonSolverConfig {
     double line_search_beta = 0.5;
     bool reuse_tangent = false;       // not used: the tangent is rebuilt every iteration
     bool verbose = true;
-    double energy_convergence_tol = 1e-2;  // not used (see DESIGN: residual tests only)
+    double energy_convergence_tol = 1e-2;  // not used: the stop tests are on the residual
     // B200 additions
     double inner_tol = 1e-12;         // PCG tolerance of each Newton correction
     int max_pcg = 5000;
@@ -235,25 +237,53 @@ struct NewtonSolverResult {
     double final_residual_relative = 0;
     double final_energy_change = 0;
     int pcg_iterations = 0;
-    std::vector<double> residual_history;
-    std::vector<double> step_size_history;
-    std::vector<double> energy_history;
+    std::vector<double> residual_history;   // ||R|| before each solve
+    std::vector<double> step_size_history;  // alpha of each accepted step
+    std::vector<double> energy_history;     // not computed (empty)
 };
+
+namespace detail {
+// optional fields of a caller's config type (the reference's
+// NewtonSolverConfig has none of the B200 additions)
+template <class T, class = void>
+struct has_inner_tol : std::false_type {};
+template <class T>
+struct has_inner_tol<T, std::void_t<decltype(std::declval<const T&>().inner_tol)>>
+    : std::true_type {};
+template <class T, class = void>
+struct has_max_pcg : std::false_type {};
+template <class T>
+struct has_max_pcg<T, std::void_t<decltype(std::declval<const T&>().max_pcg)>>
+    : std::true_type {};
+template <class T, class = void>
+struct has_precision : std::false_type {};
+template <class T>
+struct has_precision<T, std::void_t<decltype(std::declval<const T&>().precision)>>
+    : std::true_type {};
+}  // namespace detail
 
 // NonlinearNewtonSolver with the engine's mathematics: element tangent and
 // force of tet_element_stiffness_rigorous, CSR assembly, elimination BCs,
 // ILU(0)-PCG corrections, Armijo backtracking on ||R|| with
-// (1 - 0.1 alpha) as the stub's line search (:156-187).  The constrained DOFs
-// of u are set to load.load_factor * value before the iterations.
-template <class Mesh>
+// (1 - 0.1 alpha) and up to max_line_search trials, as the reference's
+// solve() (:156-187).  The constrained DOFs of u are set to
+// load.load_factor * value before the iterations.
+// Mesh, Material, BCs, load and config are templates: the reference's own
+// atlas::fem::MeshTopology, NeoHookeanMaterial (.params.E, .params.nu),
+// BoundaryConditions (.dirichlet_bcs), LoadStep (.load_factor) and
+// NewtonSolverConfig (max_iterations, tol_absolute, tol_relative,
+// max_line_search) pass unchanged; the B200 fields of this header's
+// NewtonSolverConfig (inner_tol, max_pcg, precision) are read where present.
+template <class Mesh, class Material = NeoHookeanMaterial, class BCs = BoundaryConditions>
 class NonlinearNewtonSolver {
 public:
-    NonlinearNewtonSolver(const Mesh& mesh, const NeoHookeanMaterial& mat,
-                          const BoundaryConditions& bcs, Context* ctx = nullptr)
+    NonlinearNewtonSolver(const Mesh& mesh, const Material& mat, const BCs& bcs,
+                          Context* ctx = nullptr)
         : mesh_(mesh), material_(mat), bcs_(bcs), ctx_(ctx ? ctx : &default_context()) {}
 
-    NewtonSolverResult solve(std::vector<double>& u, const LoadStep& load,
-                             const NewtonSolverConfig& config = NewtonSolverConfig()) const {
+    template <class Load, class Config = NewtonSolverConfig>
+    NewtonSolverResult solve(std::vector<double>& u, const Load& load,
+                             const Config& config = Config()) const {
         Context& ctx = *ctx_;
         set_mesh(ctx, mesh_);
         const size_t n = 3 * mesh_.nodes.size();
@@ -269,26 +299,41 @@ public:
             value[d] = std::get<2>(bc);
         }
         ctx.check(fm_set_bc(ctx.get(), mask.data(), value.data()), "fm_set_bc");
+        fm_newton_config g;
+        fm_newton_config_default(&g);
+        g.newton_rtol = config.tol_relative;
+        g.newton_atol = config.tol_absolute;
+        g.max_newton = config.max_iterations;
+        g.line_search = config.max_line_search > 0 ? config.max_line_search : 0;
+        g.ls_c = 0.1;
+        if constexpr (detail::has_inner_tol<Config>::value) g.inner_tol = config.inner_tol;
+        if constexpr (detail::has_max_pcg<Config>::value) g.max_pcg = config.max_pcg;
+        if constexpr (detail::has_precision<Config>::value) g.precision = config.precision;
+        fm_newton_result res;
+        const fm_status s = fm_newton_step_cfg_host(ctx.get(), u.data(), load.load_factor, &g,
+                                                    &res);
+        if (s != FM_OK && s != FM_ERR_NOT_CONVERGED) ctx.check(s, "fm_newton_step_cfg_host");
         NewtonSolverResult r;
-        int nit = 0, pit = 0;
-        double rel = 0.0;
-        fm_status s = fm_newton_step_host(
-            ctx.get(), u.data(), load.load_factor, config.tol_relative, config.tol_absolute,
-            config.inner_tol, config.max_iterations, config.max_pcg,
-            config.max_line_search > 0 ? config.max_line_search : 0, 0.1, config.precision, &nit,
-            &pit, &rel);
-        if (s != FM_OK && s != FM_ERR_NOT_CONVERGED) ctx.check(s, "fm_newton_step_host");
         r.converged = s == FM_OK;
-        r.num_iterations = nit;
-        r.final_residual_relative = rel;
-        r.pcg_iterations = pit;
+        r.num_iterations = res.newton_iters;
+        r.final_residual_norm = res.rnorm;
+        r.final_residual_relative = res.final_relres;
+        r.pcg_iterations = res.pcg_iters;
+        int cnt = 0;
+        fm_newton_history(ctx.get(), nullptr, 0, &cnt);
+        std::vector<fm_newton_record> h((size_t)cnt);
+        if (cnt) fm_newton_history(ctx.get(), h.data(), cnt, &cnt);
+        for (const auto& rec : h) {
+            r.residual_history.push_back(rec.rnorm);
+            if (rec.alpha > 0.0) r.step_size_history.push_back(rec.alpha);
+        }
         return r;
     }
 
 private:
     const Mesh& mesh_;
-    const NeoHookeanMaterial& material_;
-    const BoundaryConditions& bcs_;
+    const Material& material_;
+    const BCs& bcs_;
     Context* ctx_;
 };
 

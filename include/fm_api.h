@@ -47,7 +47,8 @@ typedef enum {
     FM_ERR_INVERTED = 6,       /* reserved: det F <= 0 is reported as a flag */
     FM_ERR_TIMEOUT = 7,        /* a bounded device wait expired */
     FM_ERR_NOT_CONVERGED = 8,  /* Newton/PCG stopped at its iteration cap */
-    FM_ERR_LIMITS = 9          /* mesh valence or size beyond the kernels' limits */
+    FM_ERR_LIMITS = 9,         /* mesh valence or size beyond the kernels' limits */
+    FM_ERR_DIVERGED = 10       /* Newton stopped by the divergence test */
 } fm_status;
 
 typedef enum { FM_FP64 = 0, FM_MIXED = 1 } fm_precision;
@@ -90,15 +91,32 @@ void fm_destroy(fm_ctx* ctx);
 /* Text of the last error on this context (always NUL-terminated). */
 fm_status fm_last_error(const fm_ctx* ctx, char* buf, size_t len);
 fm_status fm_get_flags(fm_ctx* ctx, uint32_t* flags);
+/* After FM_ERR_TIMEOUT the flag also stops every later wait at once (so a
+ * kernel whose dependency never arrives ends quickly): clear it before the
+ * next solve. */
 fm_status fm_clear_flags(fm_ctx* ctx);
+/* Bounded device waits (no reference counterpart: the reference's solves are
+ * serial loops).  Every dependency wait of the context's kernels (ILU(0)
+ * factorization, triangular solves) gives up after `cycles` SM clock cycles
+ * without progress, raises FM_FLAG_TIMEOUT and lets its kernel finish; the
+ * call then returns FM_ERR_TIMEOUT and the context stays usable.  cycles is
+ * rounded up to a multiple of 1024; 0 restores the default 2e9 cycles
+ * (about 1 s at B200 clocks). */
+fm_status fm_set_wait_limit(fm_ctx* ctx, uint64_t cycles);
+/* Health check of that path: one warp waits, under the context's wait
+ * limit, on a device flag that nothing sets, and the call returns
+ * FM_ERR_TIMEOUT (FM_FLAG_TIMEOUT raised) once the limit has passed. */
+fm_status fm_check_wait(fm_ctx* ctx);
 /* Size queries after fm_set_mesh: DOFs, CSR nonzeros, node neighbours. */
 fm_status fm_sizes(const fm_ctx* ctx, uint32_t* n_nodes, uint32_t* n_elems, uint32_t* n_dofs,
                    uint64_t* nnz);
 /* Built-in profiler (no reference counterpart; the reference times whole
  * phases with wall clocks, FEM/adaptive_fem_engine.hpp:1251-1273).
- * fm_profile_enable(ctx, 1) zeroes the counters and records a CUDA event
- * pair around every kernel group launched afterwards; fm_profile_read
- * synchronizes the stream and returns the totals. */
+ * Launch groups and kernel launches are always counted per class;
+ * fm_profile_enable(ctx, on) zeroes all counters, and with on = 1 also
+ * records a CUDA event pair around every kernel group launched afterwards
+ * (device time per class).  fm_profile_read synchronizes the stream and
+ * returns the totals. */
 fm_status fm_profile_enable(fm_ctx* ctx, int on);
 fm_status fm_profile_read(fm_ctx* ctx, fm_profile* out);
 
@@ -199,11 +217,12 @@ fm_status fm_ilu0_apply(fm_ctx* ctx, const double* r_dev, double* y_dev);
  * (FM_NOALLOC_MAX_DOFS doubles = 8 MiB, held by every GPU that loads the
  * library until exit), not in context buffers.  Meshes with more than
  * FM_NOALLOC_MAX_DOFS DOFs are rejected with FM_ERR_LIMITS.  The first call
- * on a device looks the array up (cudaGetSymbolAddress): make that first
- * call before any stream capture.  Every context on a device shares the
- * array: calls that overlap on the GPU race, so issue one at a time per
- * device.  Output is bit-identical to fm_ilu0_apply's.  Synchronizes the
- * context's stream. */
+ * on a device looks the array up (cudaGetSymbolAddress, with that device
+ * made current for the lookup and the caller's current device restored).
+ * Every context on a device shares the array: calls that overlap on the GPU
+ * race, so issue one at a time per device.  Output is bit-identical to
+ * fm_ilu0_apply's.  Every call synchronizes the context's stream to read the
+ * wait status, so no call can be made while that stream is capturing. */
 #define FM_NOALLOC_MAX_DOFS (1u << 20)
 fm_status fm_ilu0_apply_noalloc(fm_ctx* ctx, const double* r_dev, double* y_dev);
 
@@ -240,7 +259,10 @@ fm_status fm_csr_ilu0(fm_ctx* ctx, uint32_t n, const uint32_t* row_ptr, const ui
  * of this call).  line_search > 0 enables Armijo backtracking on ||R||
  * (accept alpha when ||R(u + alpha du)|| <= (1 - ls_c alpha) ||R(u)||,
  * alpha halved up to line_search times; FEM/adaptive_fem_engine.hpp:933-985
- * with ls_c = 1e-4, FEM/nonlinear_solver.hpp:156-187 with ls_c = 0.1). */
+ * with ls_c = 1e-4, FEM/nonlinear_solver.hpp:156-187 with ls_c = 0.1).
+ * Equals fm_newton_step_cfg with fm_newton_config_default's divergence test
+ * (growth > 10x stops with FM_ERR_DIVERGED; the slow-rate count is off),
+ * predictor_tol = inner_tol and the line search given here. */
 fm_status fm_newton_step(fm_ctx* ctx, double* u_dev, double load_frac, double newton_rtol,
                          double newton_atol, double inner_tol, int max_newton, int max_pcg,
                          int line_search, double ls_c, fm_precision prec, int* newton_iters,
@@ -255,13 +277,105 @@ fm_status fm_newton_step_host(fm_ctx* ctx, double* u_host, double load_frac, dou
                               int line_search, double ls_c, fm_precision prec, int* newton_iters,
                               int* pcg_iters, double* final_relres);
 
+/* ---- Newton configuration, result and per-iteration history ---------------
+ * fm_newton_config gathers NewtonSolverConfig (FEM/nonlinear_solver.hpp:23-34)
+ * and the Newton fields of AdaptiveFEMEngine::Config
+ * (FEM/adaptive_fem_engine.hpp:2306-2324); fm_newton_config_default fills
+ * the defaults below.
+ *   predictor_tol  PCG tolerance of the load step's Dirichlet predictor
+ *                  solve (<= 0: inner_tol).  The predictor carries the whole
+ *                  prescribed increment into the body, so an inexact
+ *                  predictor leaves it in the elements next to the loaded
+ *                  face.
+ *   line_search    Armijo backtracking as armijo_line_search_true
+ *                  (FEM/adaptive_fem_engine.hpp:933-985): alpha = 1, 1/2, ...
+ *                  accepted when ||R(u + alpha du)|| <= (1 - ls_c alpha)
+ *                  ||R(u)|| + 1e-14, at most line_search trials; when none
+ *                  is accepted alpha = 2^-line_search ("best effort").
+ *   divergence     the reference's test (:2561-2572): from the fourth
+ *                  iteration on, rate = ||R|| / ||R_prev||; rate >
+ *                  diverge_rate counts a slow iteration; stop when more than
+ *                  diverge_count were slow or when ||R|| > diverge_growth *
+ *                  ||R_prev||.  diverge_rate <= 0 or diverge_growth <= 0
+ *                  turns that half off.  Where the reference breaks out of
+ *                  the load step silently, the call returns FM_ERR_DIVERGED.
+ *   inner_tol_min  > 0: when an iteration fails to reduce ||R|| by
+ *                  diverge_rate the next corrections use a 10x tighter inner
+ *                  tolerance, down to inner_tol_min (no reference
+ *                  counterpart: the reference's inner solve is tight). */
+/* Defaults (fm_newton_config_default): newton_rtol 1e-10, newton_atol 0,
+ * inner_tol 1e-12, predictor_tol 0 (= inner_tol), inner_tol_min 0 (off),
+ * max_newton 200, max_pcg 5000, line_search 10 with ls_c 1e-4 (the engine's
+ * armijo_line_search_true(..., line_search_c = 1e-4, 10), :2314, :2581),
+ * diverge_rate 0 (off), diverge_count 3, diverge_growth 10, FP64. */
+typedef struct {
+    double newton_rtol;    /* stop when ||R|| < newton_rtol ||R_0|| */
+    double newton_atol;    /* ... or ||R|| < newton_atol */
+    double inner_tol;      /* PCG tolerance of the Newton corrections */
+    double predictor_tol;  /* PCG tolerance of the Dirichlet predictor (<= 0: inner_tol) */
+    double inner_tol_min;  /* adaptive inner tolerance floor (<= 0: fixed inner_tol) */
+    int max_newton;        /* Newton iterations per load step (predictor included) */
+    int max_pcg;           /* PCG iterations per solve */
+    int line_search;       /* Armijo trials (0: full steps) */
+    double ls_c;           /* Armijo constant */
+    double diverge_rate;   /* slow-iteration rate (reference 0.9; <= 0: off) */
+    int diverge_count;     /* slow iterations tolerated (reference 3) */
+    double diverge_growth; /* growth factor that stops at once (reference 10; <= 0: off) */
+    int precision;         /* fm_precision */
+} fm_newton_config;
+
+typedef struct {
+    int newton_iters;      /* predictor + Newton iterations */
+    int pcg_iters;         /* PCG iterations over all solves */
+    int backtracks;        /* Armijo halvings over all iterations */
+    uint32_t flags;        /* device flags (FM_FLAG_*) at exit */
+    double rnorm0;         /* ||R_0||: the predictor's right-hand side, else the first ||R|| */
+    double rnorm;          /* ||R|| at exit */
+    double final_relres;   /* rnorm / rnorm0 */
+} fm_newton_result;
+
+/* One entry per solve of the latest fm_newton_step(_cfg) call on the
+ * context, the data the reference prints per Newton iteration
+ * (FEM/adaptive_fem_engine.hpp:2548-2550).  kind 0: the Dirichlet
+ * predictor (rnorm = norm of its right-hand side), 1: a Newton iteration. */
+typedef struct {
+    int kind;
+    int pcg_iters;
+    double rnorm;          /* ||R|| before the solve (free DOFs) */
+    double alpha;          /* step length taken */
+    double inner_tol;      /* PCG tolerance used */
+    uint32_t flags;        /* device flags after this iteration's assembly */
+    uint32_t pad;
+} fm_newton_record;
+
+fm_status fm_newton_config_default(fm_newton_config* cfg);
+/* fm_newton_step with a configuration; result (nullable) filled on every
+ * return, also on FM_ERR_NOT_CONVERGED / FM_ERR_DIVERGED / FM_ERR_NONFINITE. */
+fm_status fm_newton_step_cfg(fm_ctx* ctx, double* u_dev, double load_frac,
+                             const fm_newton_config* cfg, fm_newton_result* result);
+/* Host-buffer form of fm_newton_step_cfg (u_host copied in and out inside
+ * the call, as fm_newton_step_host). */
+fm_status fm_newton_step_cfg_host(fm_ctx* ctx, double* u_host, double load_frac,
+                                  const fm_newton_config* cfg, fm_newton_result* result);
+/* Copies up to cap records of the latest Newton call; *count = records kept
+ * (at most 4096 per call). */
+fm_status fm_newton_history(const fm_ctx* ctx, fm_newton_record* out, int cap, int* count);
+
+/* fm_newton_step_cfg over load steps first_step..n_load_steps (load
+ * fraction s / n_load_steps); result totals the counts, its norms are the
+ * last step's.  A step that hits max_newton does not stop the path (the
+ * call returns FM_ERR_NOT_CONVERGED at the end); any other error does. */
+fm_status fm_newton_solve_cfg(fm_ctx* ctx, double* u_dev, int first_step, int n_load_steps,
+                              const fm_newton_config* cfg, fm_newton_result* result);
+
 /* fm_newton_solve: load steps first_step..n_load_steps of a load path.
  * Replaces NonlinearNewtonSolver::solve (FEM/nonlinear_solver.hpp:87-238)
  * with the engine's mathematics (FEM/adaptive_fem_engine.hpp:2476-2592):
  * for load step s = 1..n_load_steps the constrained DOFs of u are set to
  * (s/n) * value; then repeat {assemble, eliminate, R = -f_int,
  * stop when ||R|| < newton_rtol * ||R at the step's first iteration||
- * (or < newton_atol), ILU(0), PCG to inner_tol, u += du}.
+ * (or < newton_atol), ILU(0), PCG to inner_tol, u += alpha du with the
+ * engine's Armijo line search (10 trials, c = 1e-4, :2581)}.
  * FM_MIXED: tangent, ILU(0) and PCG in FP32; det F, ln J, f_int, R and u in
  * FP64 (the Newton loop is the iterative refinement).
  * newton_iters/pcg_iters (nullable) receive totals over all steps. */

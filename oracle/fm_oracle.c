@@ -681,12 +681,41 @@ done:
 /* Newton counts include the predictor solve.                          */
 /* Returns 0 on convergence of every step, 1 otherwise.                */
 /* ------------------------------------------------------------------ */
-int orc_newton(uint32_t n_nodes, uint32_t n_elems, const double* xyz, const uint32_t* conn,
-               const uint8_t* active, const double* mu_e, const double* lam_e, double nu,
-               const uint32_t* row_ptr, const uint32_t* col_idx, const int32_t* slot,
-               const uint8_t* mask, const double* bc_value, int n_steps, double rtol,
-               double inner_tol, int max_newton, int max_pcg, double* u, int* newton_per_step,
-               int* pcg_per_step) {
+/* Free-DOF 2-norm of R = -f (constrained entries zero) */
+static double orc_free_norm(uint32_t n, const double* f, const uint8_t* mask) {
+    double s = 0.0;
+    for (uint32_t i = 0; i < n; ++i)
+        if (!mask[i]) s += f[i] * f[i];
+    return sqrt(s);
+}
+
+/* Newton load steps first_step..last_step of an n_steps path, with the
+ * options of the GPU path's fm_newton_config:
+ *  - each load step starts with the linearized Dirichlet predictor
+ *    K_ff du_f = -f_f - K_fc v_c (v: the prescribed increment), solved to
+ *    predictor_tol (<= 0: inner_tol);
+ *  - Newton iterations: assemble, eliminate, R = -f, stop at
+ *    ||R|| < rtol ||R_0||, PCG to inner_tol, u += alpha du;
+ *  - line_search > 0: alpha from armijo_line_search_true
+ *    (FEM/adaptive_fem_engine.hpp:933-985): alpha = 1, 1/2, ... accepted
+ *    when ||R(u + alpha du)|| <= (1 - ls_c alpha) ||R(u)|| + 1e-14 (residual
+ *    re-assembled at each trial), 2^-line_search when none is accepted;
+ *  - the reference's divergence test (:2561-2572), from the fourth
+ *    iteration of a step on: rate = ||R|| / ||R_prev|| > diverge_rate counts
+ *    a slow iteration; stop when more than diverge_count were slow or
+ *    ||R|| > diverge_growth ||R_prev|| (<= 0 disables each half).
+ * Returns 0, 1 (a step hit max_newton) or 2 (the divergence test stopped a
+ * step; the remaining steps are not run).  alpha_hist (nullable) receives the
+ * step length of every Newton iteration (predictor excluded), up to alpha_cap. */
+int orc_newton_ex(uint32_t n_nodes, uint32_t n_elems, const double* xyz, const uint32_t* conn,
+                  const uint8_t* active, const double* mu_e, const double* lam_e, double nu,
+                  const uint32_t* row_ptr, const uint32_t* col_idx, const int32_t* slot,
+                  const uint8_t* mask, const double* bc_value, int first_step, int last_step,
+                  int n_steps, double rtol, double inner_tol, double predictor_tol,
+                  int max_newton, int max_pcg, int line_search, double ls_c,
+                  double diverge_rate, int diverge_count, double diverge_growth, double* u,
+                  int* newton_per_step, int* pcg_per_step, double* alpha_hist, int alpha_cap,
+                  int* n_alpha) {
     const uint32_t n = 3 * n_nodes;
     const uint64_t nnz = row_ptr[n];
     double* K = (double*)malloc(sizeof(double) * nnz);
@@ -694,11 +723,13 @@ int orc_newton(uint32_t n_nodes, uint32_t n_elems, const double* xyz, const uint
     double* R = (double*)malloc(sizeof(double) * n);
     double* du = (double*)malloc(sizeof(double) * n);
     double* v = (double*)malloc(sizeof(double) * n);
-    int status = 0;
-    for (int s = 1; s <= n_steps; ++s) {
+    double* ut = (double*)malloc(sizeof(double) * n);
+    int status = 0, na = 0;
+    const double ptol = predictor_tol > 0.0 ? predictor_tol : inner_tol;
+    for (int s = first_step; s <= last_step && status != 2; ++s) {
         double frac = (double)s / (double)n_steps;
-        double r0 = 0.0;
-        int it = 0, pcg_total = 0, conv = 0, have_r0 = 0;
+        double r0 = 0.0, r_prev = 0.0;
+        int it = 0, pcg_total = 0, conv = 0, have_r0 = 0, slow = 0;
         int any = 0;
         for (uint32_t i = 0; i < n; ++i) {
             v[i] = mask[i] ? frac * bc_value[i] - u[i] : 0.0;
@@ -713,8 +744,9 @@ int orc_newton(uint32_t n_nodes, uint32_t n_elems, const double* xyz, const uint
             r0 = sqrt(r0);
             have_r0 = 1;
             memset(du, 0, sizeof(double) * n);
-            pcg_total += orc_pcg_ilu0(n, row_ptr, col_idx, K, R, du, inner_tol, max_pcg, NULL);
+            pcg_total += orc_pcg_ilu0(n, row_ptr, col_idx, K, R, du, ptol, max_pcg, NULL);
             for (uint32_t i = 0; i < n; ++i) u[i] = mask[i] ? frac * bc_value[i] : u[i] + du[i];
+            r_prev = r0;
             it = 1;
         }
         for (; it < max_newton; ++it) {
@@ -726,16 +758,51 @@ int orc_newton(uint32_t n_nodes, uint32_t n_elems, const double* xyz, const uint
             rn = sqrt(rn);
             if (!have_r0) { r0 = rn; have_r0 = 1; }
             if (rn == 0.0 || rn < rtol * r0) { conv = 1; break; }
+            if (it > 2) {
+                const double rate = rn / (r_prev > 1e-30 ? r_prev : 1e-30);
+                if (diverge_rate > 0.0 && rate > diverge_rate) ++slow;
+                if ((diverge_rate > 0.0 && slow > diverge_count) ||
+                    (diverge_growth > 0.0 && rn > r_prev * diverge_growth)) {
+                    status = 2;
+                    break;
+                }
+            }
             memset(du, 0, sizeof(double) * n);
             pcg_total += orc_pcg_ilu0(n, row_ptr, col_idx, K, R, du, inner_tol, max_pcg, NULL);
-            for (uint32_t i = 0; i < n; ++i) u[i] += du[i];
+            double alpha = 1.0;
+            if (line_search > 0) {
+                for (int bt = 0; bt < line_search; ++bt) {
+                    for (uint32_t i = 0; i < n; ++i) ut[i] = u[i] + alpha * du[i];
+                    orc_assemble(n_nodes, n_elems, xyz, conn, active, mu_e, lam_e, nu, ut, NULL, 0,
+                                 NULL, f);
+                    if (orc_free_norm(n, f, mask) <= (1.0 - ls_c * alpha) * rn + 1e-14) break;
+                    alpha *= 0.5;
+                }
+            }
+            for (uint32_t i = 0; i < n; ++i) u[i] += alpha * du[i];
+            if (alpha_hist && na < alpha_cap) alpha_hist[na] = alpha;
+            ++na;
+            r_prev = rn;
         }
-        if (!conv) status = 1;
-        if (newton_per_step) newton_per_step[s - 1] = it;
-        if (pcg_per_step) pcg_per_step[s - 1] = pcg_total;
+        if (!conv && status != 2) status = 1;
+        if (newton_per_step) newton_per_step[s - first_step] = it;
+        if (pcg_per_step) pcg_per_step[s - first_step] = pcg_total;
     }
-    free(K); free(f); free(R); free(du); free(v);
+    if (n_alpha) *n_alpha = na;
+    free(K); free(f); free(R); free(du); free(v); free(ut);
     return status;
+}
+
+int orc_newton(uint32_t n_nodes, uint32_t n_elems, const double* xyz, const uint32_t* conn,
+               const uint8_t* active, const double* mu_e, const double* lam_e, double nu,
+               const uint32_t* row_ptr, const uint32_t* col_idx, const int32_t* slot,
+               const uint8_t* mask, const double* bc_value, int n_steps, double rtol,
+               double inner_tol, int max_newton, int max_pcg, double* u, int* newton_per_step,
+               int* pcg_per_step) {
+    return orc_newton_ex(n_nodes, n_elems, xyz, conn, active, mu_e, lam_e, nu, row_ptr, col_idx,
+                         slot, mask, bc_value, 1, n_steps, n_steps, rtol, inner_tol, 0.0,
+                         max_newton, max_pcg, 0, 0.0, 0.0, 0, 0.0, u, newton_per_step,
+                         pcg_per_step, NULL, 0, NULL);
 }
 
 /* ------------------------------------------------------------------ */

@@ -79,6 +79,12 @@ def lib():
                                  _u32p, _u32p, _i32p, _u8p, _f64p, i32, f64, f64, i32, i32,
                                  _f64p, _opt(_i32p), _opt(_i32p)]
         L.orc_newton.restype = i32
+        L.orc_newton_ex.argtypes = [u32, u32, _f64p, _u32p, _opt(_u8p), _f64p, _f64p, f64,
+                                    _u32p, _u32p, _i32p, _u8p, _f64p, i32, i32, i32, f64, f64,
+                                    f64, i32, i32, i32, f64, f64, i32, f64, _f64p,
+                                    _opt(_i32p), _opt(_i32p), _opt(_f64p), i32,
+                                    C.POINTER(i32)]
+        L.orc_newton_ex.restype = i32
         L.orc_exact_apply.argtypes = [u32, u32, _f64p, _u32p, _opt(_u8p), _f64p, _f64p,
                                       _f64p, _f64p, _f64p, i32]
         L.orc_param_grads.argtypes = [u32, _f64p, _u32p, _opt(_u8p), _f64p, _f64p, _f64p, _f64p]
@@ -266,6 +272,31 @@ def newton(xyz, conn, mu_e, lam_e, nu, rp, ci, slot, mask, bc_value, n_steps, rt
                           np.ascontiguousarray(bc_value, np.float64), n_steps, rtol, inner_tol,
                           max_newton, max_pcg, u, nps, pps)
     return u, st, nps, pps
+
+
+def newton_ex(xyz, conn, mu_e, lam_e, nu, rp, ci, slot, mask, bc_value, n_steps, first_step=1,
+              last_step=None, rtol=1e-10, inner_tol=1e-12, predictor_tol=0.0, max_newton=200,
+              max_pcg=5000, line_search=0, ls_c=1e-4, diverge_rate=0.0, diverge_count=3,
+              diverge_growth=0.0, u0=None, active=None, alpha_cap=100000):
+    """orc_newton_ex: load steps first_step..last_step with the GPU path's
+    Newton options; returns (u, status, newton per step, pcg per step,
+    alpha of every Newton iteration)"""
+    nn = xyz.size // 3
+    ne = conn.size // 4
+    last_step = n_steps if last_step is None else last_step
+    k = last_step - first_step + 1
+    u = np.zeros(3 * nn, np.float64) if u0 is None else np.array(u0, np.float64)
+    nps = np.zeros(k, np.int32)
+    pps = np.zeros(k, np.int32)
+    al = np.zeros(alpha_cap, np.float64)
+    na = C.c_int()
+    st = lib().orc_newton_ex(nn, ne, xyz, conn, active, np.ascontiguousarray(mu_e, np.float64),
+                             np.ascontiguousarray(lam_e, np.float64), nu, rp, ci, slot, mask,
+                             np.ascontiguousarray(bc_value, np.float64), first_step, last_step,
+                             n_steps, rtol, inner_tol, predictor_tol, max_newton, max_pcg,
+                             line_search, ls_c, diverge_rate, diverge_count, diverge_growth, u,
+                             nps, pps, al, alpha_cap, C.byref(na))
+    return u, st, nps, pps, al[:min(na.value, alpha_cap)]
 
 
 def exact_apply(xyz, conn, mu_e, lam_e, u, v, transpose=False, active=None):

@@ -1,0 +1,144 @@
+"""The scale-up workload's complete load path, shrunk to 16^3 x 6 tets, and
+the Newton loop's safeguards, GPU (through the C ABI) against the oracle.
+
+- FP64, the reference's Newton loop with Armijo backtracking on every
+  iteration (armijo_line_search_true, FEM/adaptive_fem_engine.hpp:933-985,
+  c = 1e-4, 10 trials): Newton counts per load level and every step length
+  equal to the oracle's, u after levels 5 and 10 within 1e-10 relative
+  (tests/golden/scaleup16_path.npz, made by tests/golden/make_scaleup_path.py).
+- Mixed precision at the benchmark's settings (FP32 tangent/ILU(0)/PCG to
+  0.2, FP64 residual): u after level 10 within 1e-8 of the FP64 oracle.
+- Armijo on a step whose full Newton steps fail: the same backtracking
+  sequence and iterate as the oracle.
+- The reference's divergence test (:2561-2572, rate > 0.9 more than 3 times)
+  stops at the same iteration as in the oracle, with FM_ERR_DIVERGED.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TOL_U = 1e-10     # FP64 GPU vs FP64 oracle, relative 2-norm
+TOL_MIXED = 1e-8  # mixed GPU vs FP64 oracle, relative 2-norm
+FM_ERR_NOT_CONVERGED, FM_ERR_DIVERGED = 8, 10
+
+
+@pytest.fixture(scope="module")
+def fm():
+    import flexmesh_b200 as F
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return F
+
+
+@pytest.fixture(scope="module")
+def path16():
+    return np.load(os.path.join(HERE, "golden", "scaleup16_path.npz"))
+
+
+def scaleup_ctx(fm, N=16):
+    from flexmesh_b200 import configs
+
+    P = configs.scaleup_block(N)
+    ctx = fm.Context(0)
+    ctx.set_mesh(P.xyz, P.conn, P.elem_volume)
+    ctx.set_material(P.E, P.nu, P.E_elem)
+    ctx.set_bc(P.mask, P.bc_value)
+    return ctx, P
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def alphas_of(hist):
+    return [h["alpha"] for h in hist if h["kind"] == 1 and h["alpha"] > 0]
+
+
+def test_scaleup16_path_fp64_matches_oracle(fm, path16):
+    ctx, P = scaleup_ctx(fm)
+    u = torch.zeros(P.xyz.size, dtype=torch.float64, device="cuda")
+    newton, alphas = [], []
+    for s in range(1, P.n_steps + 1):
+        r = ctx.newton_step_cfg(u, s / P.n_steps, newton_rtol=1e-10, inner_tol=1e-12,
+                                max_newton=400, max_pcg=20000, line_search=10, ls_c=1e-4,
+                                prec=fm.FM_FP64)
+        newton.append(r["newton_iters"])
+        alphas.extend(alphas_of(ctx.newton_history()))
+        if s == 5:
+            assert rel(u.cpu().numpy(), path16["u_level5"]) <= TOL_U
+    assert newton == path16["newton"].tolist()
+    assert np.array_equal(np.array(alphas), path16["alpha"])
+    assert (path16["alpha"] < 1).any()  # the path does backtrack (levels 8-10)
+    assert rel(u.cpu().numpy(), path16["u_level10"]) <= TOL_U
+
+
+def test_scaleup16_path_mixed_within_1e8(fm, path16):
+    ctx, P = scaleup_ctx(fm)
+    u = torch.zeros(P.xyz.size, dtype=torch.float64, device="cuda")
+    for s in range(1, P.n_steps + 1):
+        ctx.newton_step_cfg(u, s / P.n_steps, newton_rtol=1e-10, inner_tol=0.2,
+                            predictor_tol=1e-6, max_newton=400, max_pcg=20000, line_search=10,
+                            ls_c=1e-4, prec=fm.FM_MIXED)
+    assert rel(u.cpu().numpy(), path16["u_level10"]) <= TOL_MIXED
+
+
+def one_step_case(N=4, uz=-0.5):
+    from flexmesh_b200 import configs
+
+    return configs.unit_cube_problem("big-step", N, sigma_log=0.3, uz_total=uz, n_steps=1)
+
+
+def oracle_run(P, **kw):
+    rp, ci = O.pattern(P.n_nodes, P.conn, "solve")
+    mu, lam = P.lame()
+    return O.newton_ex(P.xyz, P.conn, mu, lam, P.nu, rp, ci,
+                       O.slot_map(P.n_nodes, P.conn, rp, ci), P.mask, P.bc_value, 1,
+                       active=(P.elem_volume >= 1e-30).astype(np.uint8), **kw)
+
+
+def test_armijo_backtracks_as_oracle(fm):
+    """u_z = -0.5 in one load step on 4^3 x 6 tets: full Newton steps fail,
+    the line search halves down to 2^-10; 12 iterations, same alphas and
+    iterate as the oracle"""
+    P = one_step_case()
+    ctx = fm.Context(0)
+    ctx.set_mesh(P.xyz, P.conn, P.elem_volume)
+    ctx.set_material(P.E, P.nu, P.E_elem)
+    ctx.set_bc(P.mask, P.bc_value)
+    u = torch.zeros(P.xyz.size, dtype=torch.float64, device="cuda")
+    r = ctx.newton_step_cfg(u, 1.0, newton_rtol=1e-10, inner_tol=1e-12, max_newton=12,
+                            line_search=10, ls_c=1e-4, diverge_growth=0.0, prec=fm.FM_FP64,
+                            allow=(FM_ERR_NOT_CONVERGED,))
+    uo, st, nps, _, al = oracle_run(P, rtol=1e-10, inner_tol=1e-12, max_newton=12,
+                                    line_search=10, ls_c=1e-4)
+    assert r["status"] == FM_ERR_NOT_CONVERGED and st == 1
+    a = alphas_of(ctx.newton_history())
+    assert a == al.tolist()
+    assert min(a) < 0.01 and r["backtracks"] == sum(int(round(-np.log2(x))) for x in a)
+    assert rel(u.cpu().numpy(), uo) <= TOL_U
+
+
+def test_reference_divergence_test_stops_as_oracle(fm):
+    P = one_step_case()
+    ctx = fm.Context(0)
+    ctx.set_mesh(P.xyz, P.conn, P.elem_volume)
+    ctx.set_material(P.E, P.nu, P.E_elem)
+    ctx.set_bc(P.mask, P.bc_value)
+    u = torch.zeros(P.xyz.size, dtype=torch.float64, device="cuda")
+    r = ctx.newton_step_cfg(u, 1.0, newton_rtol=1e-10, inner_tol=1e-12, max_newton=100,
+                            line_search=0, diverge_rate=0.9, diverge_count=3,
+                            diverge_growth=10.0, prec=fm.FM_FP64, allow=(FM_ERR_DIVERGED,))
+    uo, st, nps, _, _ = oracle_run(P, rtol=1e-10, inner_tol=1e-12, max_newton=100,
+                                   diverge_rate=0.9, diverge_count=3, diverge_growth=10.0)
+    assert r["status"] == FM_ERR_DIVERGED and st == 2
+    assert "diverging" in r["error"]
+    assert r["newton_iters"] == int(nps[0])
+    assert rel(u.cpu().numpy(), uo) <= TOL_U
