@@ -154,6 +154,9 @@ struct fm_ctx {
 
     // per-solve records of the latest Newton call (fm_newton_history)
     std::vector<fm_newton_record> newton_hist;
+    // element state arrays updated after every Newton update of u (nullable)
+    double* state_F = nullptr;
+    double* state_stress = nullptr;
 
     unsigned* status() { return &sc.p->status; }
     unsigned* counter() { return &sc.p->counter[0]; }
@@ -1303,6 +1306,15 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
         return FM_OK;
     };
 
+    // the engine updates the element states after every Newton update of u
+    // (FEM/adaptive_fem_engine.hpp:2589); here when state arrays are attached
+    auto update_states = [&]() {
+        if (!c->state_F || !c->state_stress) return;
+        PROF(FM_PROF_STATES, 1);
+        fm::launch_element_states(m, u, c->nu, c->state_F, c->state_stress,
+                                  &c->sc.p->state_violations, c->status(), c->stream);
+    };
+
     auto finish = [&](fm_status st) -> fm_status {
         c->w64.factor_valid = c->w32.factor_valid = false;
         if (res) {
@@ -1358,6 +1370,7 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
         }
         { PROF(FM_PROF_VECTOR, 1); fm::launch_set_bc_values(c->n, c->mask.p, c->has_bcval ? c->bcval.p : nullptr, load_frac,
                                  u, c->stream); }
+        update_states();
     }
 
     bool conv = false;
@@ -1431,6 +1444,7 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
             TRY(sync_scalars(c));
         }
         CK(cudaGetLastError());
+        update_states();
         n_pcg += its;
         ++n_newton;
         record(1, its, rn, alpha, tol);
@@ -1445,6 +1459,31 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
                            flags_text(c->h_sc->status).c_str()));
     }
     return finish(out);
+}
+
+fm_status fm_element_states(fm_ctx* c, const double* u, double* F, double* stress,
+                            uint32_t* det_violations) {
+    TRY(need_material(c));
+    if (!u || !F || !stress) return fail(c, FM_ERR_ARG, "null argument");
+    CK(cudaMemsetAsync(&c->sc.p->state_violations, 0, sizeof(unsigned), c->stream));
+    {
+        PROF(FM_PROF_STATES, 1);
+        fm::launch_element_states(mesh_view(c), u, c->nu, F, stress, &c->sc.p->state_violations,
+                                  c->status(), c->stream);
+    }
+    CK(cudaGetLastError());
+    TRY(sync_scalars(c));
+    if (det_violations) *det_violations = c->h_sc->state_violations;
+    return check_flags(c, c->h_sc->status, "fm_element_states");
+}
+
+fm_status fm_set_state_output(fm_ctx* c, double* F, double* stress) {
+    TRY(need_mesh(c));
+    if ((F == nullptr) != (stress == nullptr))
+        return fail(c, FM_ERR_ARG, "give both state arrays or neither");
+    c->state_F = F;
+    c->state_stress = stress;
+    return FM_OK;
 }
 
 fm_status fm_newton_history(const fm_ctx* c, fm_newton_record* out, int cap, int* count) {

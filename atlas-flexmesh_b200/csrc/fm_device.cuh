@@ -39,6 +39,7 @@ struct DevScalars {
     unsigned wait_budget;  // bounded-wait limit in 1024 cycles (0: kWaitCycles); follows status
     unsigned counter[8];  // last-block counters (one per reduction site)
     unsigned never;       // a flag no kernel sets (fm_check_wait waits on it)
+    unsigned state_violations;  // element state update: |det F_sl3 - 1| > 1e-8 count
 };
 
 constexpr int kRedBlocks = 296;  // 2 x 148 SMs: fixed grid => fixed summation order
@@ -238,7 +239,8 @@ __device__ __forceinline__ void grad_of(const TetKin& k, int a, double g[3]) {
 // (neo_hookean_response, FEM/adaptive_fem_engine.hpp:79-129), evaluated in
 // the closed form M = mu (C - I) + lam lnJ I that C C^-1 = I gives; the
 // reference's Voigt round trip M01*sqrt2/sqrt2 is the identity up to one
-// rounding.  Out: symmetric M as (00,11,22,01,02,12) and lnJ.
+// rounding.  A degenerate C (det C = J^2 < 1e-30) takes the reference's
+// guarded inverse instead.  Out: symmetric M as (00,11,22,01,02,12) and lnJ.
 struct Mandel {
     double m00, m11, m22, m01, m02, m12;
     double lnJ;
@@ -255,6 +257,19 @@ __device__ __forceinline__ Mandel mandel_stress(const double F[9], double J, dou
     const double Js = J < kJSafe ? kJSafe : J;
     M.lnJ = log(Js);
     const double vol = lam * M.lnJ;
+    if (J * J < 1e-30) {
+        // det C = J^2 below matrix_3x3_inv's 1e-30 guard (:56-60): the
+        // reference's C^-1 is then 1e30 I, S = (mu (1 - 1e30) + lam lnJ 1e30) I
+        // and M = C S
+        const double s = mu * (1.0 - 1e30) + vol * 1e30;
+        M.m00 = s * c00;
+        M.m11 = s * c11;
+        M.m22 = s * c22;
+        M.m01 = s * c01;
+        M.m02 = s * c02;
+        M.m12 = s * c12;
+        return M;
+    }
     M.m00 = mu * (c00 - 1.0) + vol;
     M.m11 = mu * (c11 - 1.0) + vol;
     M.m22 = mu * (c22 - 1.0) + vol;

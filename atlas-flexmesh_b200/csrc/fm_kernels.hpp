@@ -142,6 +142,13 @@ void launch_apply_bc_nodes(uint32_t nn, const uint32_t* nbr_ptr, const uint32_t*
 // y = scale * x (FP32 -> FP64)
 void launch_f32_to_f64_scaled(uint32_t n, const float* x, double scale, double* y,
                               cudaStream_t s);
+// Element state update (fm_states.cu): per element F_sl3 (9, the
+// reference's column-major Matrix3x3 data) and Mandel stress (6); elements
+// with a degenerate reference Jacobian keep their previous state.
+// violations (nullable) counts |det F_sl3 - 1| > 1e-8.
+void launch_element_states(const MeshDev& m, const double* u, double nu, double* F,
+                           double* stress, unsigned* violations, unsigned* status,
+                           cudaStream_t s);
 // one warp waits (bounded by the limit that travels with status) for *flag
 // to reach epoch 1; nothing sets it, so the wait times out
 void launch_wait_probe(const unsigned* flag, unsigned* status, cudaStream_t s);

@@ -32,9 +32,9 @@ EXPORTS = [
     "fm_exact_apply", "fm_adjoint", "fm_csr_ilu0", "fm_newton_step", "fm_newton_step_host",
     "fm_profile_enable", "fm_profile_read", "fm_newton_config_default", "fm_newton_step_cfg",
     "fm_newton_history", "fm_set_wait_limit", "fm_check_wait", "fm_newton_step_cfg_host",
-    "fm_newton_solve_cfg",
+    "fm_newton_solve_cfg", "fm_element_states", "fm_set_state_output",
 ]
-PROF_KINDS = {0: "assemble", 1: "ilu0", 2: "trsv", 3: "spmv", 4: "vector"}
+PROF_KINDS = {0: "assemble", 1: "ilu0", 2: "trsv", 3: "spmv", 4: "vector", 5: "states"}
 
 
 class Profile(C.Structure):
@@ -121,6 +121,8 @@ def lib() -> C.CDLL:
             "fm_newton_history": [_vp, _P(NewtonRecord), _i32, _P(_i32)],
             "fm_newton_step_cfg_host": [_vp, _vp, _f64, _P(NewtonConfig), _P(NewtonResult)],
             "fm_newton_solve_cfg": [_vp, _vp, _i32, _i32, _P(NewtonConfig), _P(NewtonResult)],
+            "fm_element_states": [_vp, _vp, _vp, _vp, _P(_u32)],
+            "fm_set_state_output": [_vp, _vp, _vp],
             "fm_set_wait_limit": [_vp, _u64],
             "fm_check_wait": [_vp],
             "fm_profile_enable": [_vp, _i32],
@@ -456,6 +458,25 @@ class Context:
         if st and st not in allow:
             self._check(st, "fm_newton_solve_cfg")
         return out
+
+    def element_states(self, u, F=None, stress=None):
+        """fm_element_states: (F_sl3 [E, 9], stress [E, 6], det violations);
+        F/stress default to ElementState's initial values (identity, zero)"""
+        t = self.torch
+        if F is None:
+            F = t.eye(3, dtype=t.float64, device=f"cuda:{self.device}").reshape(1, 9).repeat(
+                self.n_elems, 1).contiguous()
+        if stress is None:
+            stress = self._zeros(6 * self.n_elems).view(self.n_elems, 6)
+        v = _u32()
+        self._check(lib().fm_element_states(self._h, _dp(u), _dp(F), _dp(stress), C.byref(v)),
+                    "fm_element_states")
+        return F, stress, v.value
+
+    def set_state_output(self, F=None, stress=None):
+        self._state_keep = (F, stress)  # the library holds the raw pointers
+        self._check(lib().fm_set_state_output(self._h, _dp(F), _dp(stress)),
+                    "fm_set_state_output")
 
     def newton_history(self):
         """per-solve records of the latest Newton call"""

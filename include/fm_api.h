@@ -76,6 +76,7 @@ enum {
     FM_PROF_TRSV = 2,     /* preconditioner apply: forward + backward solve */
     FM_PROF_SPMV = 3,     /* K x */
     FM_PROF_VECTOR = 4,   /* PCG/Newton vector updates and reductions */
+    FM_PROF_STATES = 5,   /* element state update */
     FM_PROF_KINDS = 8
 };
 typedef struct {
@@ -383,6 +384,28 @@ fm_status fm_newton_solve(fm_ctx* ctx, double* u_dev, int first_step, int n_load
                           double newton_rtol, double newton_atol, double inner_tol,
                           int max_newton, int max_pcg, fm_precision prec, int* newton_iters,
                           int* pcg_iters, double* final_relres);
+
+/* ---- element state update --------------------------------------------------
+ * Replaces update_element_states_rigorous (FEM/adaptive_fem_engine.hpp:
+ * 2716-2794).  For every tet whose reference Jacobian is invertible
+ * (|det| >= 1e-30, as the reference tests it): F = I + grad u,
+ * F_sl3 = sl3_retraction(F, 0) = exp(log F) rescaled to det 1
+ * (CORE/lie_operator.cpp:300), and the Neo-Hookean Mandel stress of F_sl3
+ * (neo_hookean_response, :79-129, with J = det F_sl3: the reference passes
+ * an uninitialized J there, :2784-2785).  F_dev[9e .. 9e+8]: F_sl3 as
+ * ElementState::F_data holds it; stress_dev[6e .. 6e+5]: Voigt (S11, S22,
+ * S33, sqrt2 S12, sqrt2 S13, sqrt2 S23).  Other tets keep their values
+ * (initialize them as ElementState::initialize does: F = I, stress = 0).
+ * det_violations (nullable): tets with |det F_sl3 - 1| > 1e-8, the count of
+ * RuntimeInvariantMonitor::check_sl3_element (CORE/lie_operator.hpp:244).
+ * The engine's J2 return after it (:2109) is an empty stub and not run. */
+fm_status fm_element_states(fm_ctx* ctx, const double* u_dev, double* F_dev, double* stress_dev,
+                            uint32_t* det_violations);
+/* Attach state arrays to the Newton calls: with both non-NULL every
+ * fm_newton_step(_cfg) / fm_newton_solve(_cfg) updates them after each
+ * update of u (the predictor's and every Newton iteration's), as the
+ * engine does after each Newton iteration (:2589).  NULL, NULL detaches. */
+fm_status fm_set_state_output(fm_ctx* ctx, double* F_dev, double* stress_dev);
 
 /* ---- A9/A21: exact Jacobian and adjoint (no reference counterpart) --------
  * fm_exact_apply: y = K_exact v (transpose = 0) or K_exact^T v (1), the

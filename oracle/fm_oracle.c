@@ -1004,3 +1004,227 @@ uint32_t orc_poisson(uint32_t g, uint32_t* row_ptr, uint32_t* col_idx, double* v
     orc_spmv(g * g, row_ptr, col_idx, val, x_exact, b);
     return w;
 }
+
+/* ------------------------------------------------------------------ */
+/* Element state update: update_element_states_rigorous               */
+/* (FEM/adaptive_fem_engine.hpp:2716-2794) with the SL(3) retraction  */
+/* of CORE/lie_operator.cpp (exp :95-152, Denman-Beavers square root  */
+/* :164-184, log :200-268, retraction :300-311), restated on its      */
+/* column-major Matrix3x3 data layout (a[c*3 + r]).                   */
+/* ------------------------------------------------------------------ */
+typedef struct { double a[9]; } orc_m3;
+
+static orc_m3 m3_ident(void) { orc_m3 r = {{1, 0, 0, 0, 1, 0, 0, 0, 1}}; return r; }
+static orc_m3 m3_zero(void) { orc_m3 r = {{0, 0, 0, 0, 0, 0, 0, 0, 0}}; return r; }
+static orc_m3 m3_add(orc_m3 A, orc_m3 B) { for (int i = 0; i < 9; ++i) A.a[i] = A.a[i] + B.a[i]; return A; }
+static orc_m3 m3_sub(orc_m3 A, orc_m3 B) { for (int i = 0; i < 9; ++i) A.a[i] = A.a[i] - B.a[i]; return A; }
+static orc_m3 m3_scale(orc_m3 A, double s) { for (int i = 0; i < 9; ++i) A.a[i] = A.a[i] * s; return A; }
+static orc_m3 m3_mul(orc_m3 A, orc_m3 B) {
+    orc_m3 C;
+    for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r)
+            C.a[3 * c + r] = A.a[r] * B.a[3 * c] + A.a[3 + r] * B.a[3 * c + 1] + A.a[6 + r] * B.a[3 * c + 2];
+    return C;
+}
+static double m3_trace(orc_m3 A) { return A.a[0] + A.a[4] + A.a[8]; }
+static double m3_frob(orc_m3 A) {
+    double s = 0.0;
+    for (int i = 0; i < 9; ++i) s += A.a[i] * A.a[i];
+    return sqrt(s);
+}
+static double m3_inf(orc_m3 A) {
+    double m = 0.0;
+    for (int r = 0; r < 3; ++r) {
+        double t = fabs(A.a[r]) + fabs(A.a[3 + r]) + fabs(A.a[6 + r]);
+        if (t > m) m = t;
+    }
+    return m;
+}
+static double m3_one(orc_m3 A) {
+    double m = 0.0;
+    for (int c = 0; c < 3; ++c) {
+        double t = fabs(A.a[3 * c]) + fabs(A.a[3 * c + 1]) + fabs(A.a[3 * c + 2]);
+        if (t > m) m = t;
+    }
+    return m;
+}
+static double m3_det(orc_m3 A) {
+    return A.a[0] * (A.a[4] * A.a[8] - A.a[7] * A.a[5]) - A.a[3] * (A.a[1] * A.a[8] - A.a[7] * A.a[2]) +
+           A.a[6] * (A.a[1] * A.a[5] - A.a[4] * A.a[2]);
+}
+static orc_m3 m3_inv(orc_m3 A) {
+    const double a00 = A.a[0], a10 = A.a[1], a20 = A.a[2];
+    const double a01 = A.a[3], a11 = A.a[4], a21 = A.a[5];
+    const double a02 = A.a[6], a12 = A.a[7], a22 = A.a[8];
+    const double c00 = a11 * a22 - a21 * a12, c10 = -(a01 * a22 - a21 * a02), c20 = a01 * a12 - a11 * a02;
+    const double c01 = -(a10 * a22 - a20 * a12), c11 = a00 * a22 - a20 * a02, c21 = -(a00 * a12 - a10 * a02);
+    const double c02 = a10 * a21 - a20 * a11, c12 = -(a00 * a21 - a20 * a01), c22 = a00 * a11 - a10 * a01;
+    const double d = a00 * c00 + a10 * c10 + a20 * c20;
+    if (fabs(d) < 1.0e-15) return m3_ident();
+    const double id = 1.0 / d;
+    orc_m3 r = {{c00 * id, c01 * id, c02 * id, c10 * id, c11 * id, c12 * id, c20 * id, c21 * id, c22 * id}};
+    return r;
+}
+static double m3_cond(orc_m3 A) {
+    if (fabs(m3_det(A)) < 1.0e-15) return 1.0e18;
+    double k = m3_one(A) * m3_one(m3_inv(A));
+    return k < 1.0e18 ? k : 1.0e18;
+}
+static orc_m3 m3_expm(orc_m3 A) {
+    const double b1 = 0.5, b2 = 0.1, b3 = 1.0 / 120.0, theta3 = 1.495585217958292;
+    const double nrm = m3_inf(A);
+    if (!isfinite(nrm)) return m3_ident();
+    int s = 0;
+    if (nrm > theta3) s = (int)ceil(log2(nrm / theta3));
+    if (m3_cond(A) > 1.0e8 && s < 8) ++s;
+    const double sc = 1.0 / (double)(1LL << s);
+    const orc_m3 X = m3_scale(A, sc), X2 = m3_mul(X, X), X3 = m3_mul(X2, X), I = m3_ident();
+    const orc_m3 P = m3_add(m3_add(I, m3_scale(X, b1)), m3_add(m3_scale(X2, b2), m3_scale(X3, b3)));
+    const orc_m3 Q = m3_add(m3_add(I, m3_scale(X, -b1)), m3_add(m3_scale(X2, b2), m3_scale(X3, -b3)));
+    orc_m3 R = m3_mul(m3_inv(Q), P);
+    for (int i = 0; i < s; ++i) R = m3_mul(R, R);
+    const double dR = m3_det(R), target = exp(m3_trace(A));
+    if (isfinite(dR) && isfinite(target) && dR > 1.0e-300 && target > 1.0e-300)
+        R = m3_scale(R, cbrt(target / dR));
+    return R;
+}
+static orc_m3 m3_sqrt_db(orc_m3 A) {
+    orc_m3 Y = A, Z = m3_ident();
+    for (int it = 0; it < 20; ++it) {
+        if (m3_frob(m3_sub(m3_mul(Y, Y), A)) < 4.0e-16) break;
+        const orc_m3 Yi = m3_inv(Y), Zi = m3_inv(Z);
+        const orc_m3 Yn = m3_scale(m3_add(Y, Zi), 0.5), Zn = m3_scale(m3_add(Z, Yi), 0.5);
+        Y = Yn;
+        Z = Zn;
+    }
+    return Y;
+}
+static orc_m3 m3_logm(orc_m3 A) {
+    double fs = 0.0;
+    for (int i = 0; i < 9; ++i) fs += A.a[i] * A.a[i];
+    if (!isfinite(fs)) return m3_zero();
+    const orc_m3 I = m3_ident();
+    {
+        const orc_m3 E = m3_sub(A, I);
+        if (m3_inf(E) < 1.0e-7) {
+            const orc_m3 E2 = m3_mul(E, E), E3 = m3_mul(E2, E);
+            return m3_add(m3_sub(E, m3_scale(E2, 0.5)), m3_scale(E3, 1.0 / 3.0));
+        }
+    }
+    orc_m3 B = A;
+    int roots = 0;
+    for (int k = 0; k < 16; ++k) {
+        if (m3_inf(m3_sub(B, I)) < 0.125) break;
+        B = m3_sqrt_db(B);
+        ++roots;
+    }
+    const orc_m3 Z = m3_mul(m3_sub(B, I), m3_inv(m3_add(B, I))), Z2 = m3_mul(Z, Z);
+    orc_m3 Zp = Z, sum = Z;
+    for (int k = 1; k <= 32; ++k) {
+        Zp = m3_mul(Zp, Z2);
+        sum = m3_add(sum, m3_scale(Zp, 1.0 / (double)(2 * k + 1)));
+    }
+    orc_m3 L = m3_scale(m3_scale(sum, 2.0), (double)(1LL << roots));
+    orc_m3 best = L;
+    double best_rel = INFINITY;
+    const double fa = m3_frob(A), denom = fa > 1.0e-30 ? fa : 1.0e-30;
+    for (int it = 0; it < 4; ++it) {
+        const orc_m3 eL = m3_expm(L), res = m3_sub(A, eL);
+        const double rel = m3_frob(res) / denom;
+        if (isfinite(rel) && rel < best_rel) { best_rel = rel; best = L; }
+        if (rel < 1.0e-12) break;
+        const orc_m3 corr = m3_mul(res, m3_inv(eL));
+        const double cn = m3_frob(corr);
+        if (!isfinite(cn) || cn > 0.25) break;
+        L = m3_add(L, corr);
+    }
+    return best;
+}
+
+/* sl3_retraction(G, 0): exp(log G) rescaled to det 1 */
+void orc_sl3_retraction(const double G[9], double out[9]) {
+    orc_m3 g;
+    memcpy(g.a, G, sizeof g.a);
+    orc_m3 R = m3_expm(m3_add(m3_logm(g), m3_zero()));
+    const double d = m3_det(R);
+    if (fabs(d) > 1.0e-15) R = m3_scale(R, 1.0 / cbrt(d));
+    memcpy(out, R.a, sizeof R.a);
+}
+
+/* neo_hookean_response (:79-129) with a defined J */
+void orc_nh_response(const double F[9], double mu, double lam, double J, double sig[6]) {
+    double C[9], Ci[9], S[9], M[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double s = 0.0;
+            for (int k = 0; k < 3; ++k) s += F[k * 3 + i] * F[k * 3 + j];
+            C[i * 3 + j] = s;
+        }
+    orc_inv3(C, Ci);
+    const double lnJ = log(J < 0.01 ? 0.01 : J);
+    for (int i = 0; i < 9; ++i) S[i] = mu * ((i % 4 == 0 ? 1.0 : 0.0) - Ci[i]) + lam * lnJ * Ci[i];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double s = 0.0;
+            for (int k = 0; k < 3; ++k) s += C[i * 3 + k] * S[k * 3 + j];
+            M[i * 3 + j] = s;
+        }
+    sig[0] = M[0];
+    sig[1] = M[4];
+    sig[2] = M[8];
+    sig[3] = M[1] * ORC_SQRT2;
+    sig[4] = M[2] * ORC_SQRT2;
+    sig[5] = M[5] * ORC_SQRT2;
+}
+
+/* The update of every element's state at displacement u: F_sl3 (9 per tet)
+ * and stress (6 per tet) for tets with |det J_ref| >= 1e-30; others are left
+ * as they are.  J of the stress is det F_sl3 (the reference passes an
+ * uninitialized value).  Returns the count of |det F_sl3 - 1| > 1e-8. */
+uint32_t orc_element_states(uint32_t n_nodes, uint32_t n_elems, const double* xyz,
+                            const uint32_t* conn, const double* mu_e, const double* lam_e,
+                            const double* u, double* Fst, double* stress) {
+    (void)n_nodes;
+    static const double xi[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    uint32_t bad = 0;
+    for (uint32_t e = 0; e < n_elems; ++e) {
+        const uint32_t* c = conn + 4 * (size_t)e;
+        double x[4][3], ue[4][3], J[9], Ji[9], dN[4][3], g[9];
+        for (int a = 0; a < 4; ++a)
+            for (int d = 0; d < 3; ++d) {
+                x[a][d] = xyz[3 * (size_t)c[a] + d];
+                ue[a][d] = u[3 * (size_t)c[a] + d];
+            }
+        for (int d = 0; d < 3; ++d) {
+            J[d * 3 + 0] = x[1][d] - x[0][d];
+            J[d * 3 + 1] = x[2][d] - x[0][d];
+            J[d * 3 + 2] = x[3][d] - x[0][d];
+        }
+        orc_inv3(J, Ji);
+        const double dJ = J[0] * (J[4] * J[8] - J[7] * J[5]) - J[3] * (J[1] * J[8] - J[7] * J[2]) +
+                          J[6] * (J[1] * J[5] - J[4] * J[2]);
+        if (fabs(dJ) < 1e-30) continue;
+        for (int a = 0; a < 4; ++a)
+            for (int i = 0; i < 3; ++i) {
+                double s = 0.0;
+                for (int j = 0; j < 3; ++j) s += Ji[j * 3 + i] * xi[a][j];
+                dN[a][i] = s;
+            }
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double s = 0.0;
+                for (int a = 0; a < 4; ++a) s += ue[a][i] * dN[a][j];
+                g[i * 3 + j] = s;
+            }
+        double F[9], Fs[9];
+        for (int i = 0; i < 9; ++i) F[i] = (i % 4 == 0) ? 1.0 + g[i] : g[i];
+        orc_sl3_retraction(F, Fs);
+        orc_m3 fs;
+        memcpy(fs.a, Fs, sizeof fs.a);
+        const double dF = m3_det(fs);
+        orc_nh_response(Fs, mu_e[e], lam_e[e], dF, stress + 6 * (size_t)e);
+        memcpy(Fst + 9 * (size_t)e, Fs, sizeof Fs);
+        if (fabs(dF - 1.0) > 1.0e-8) ++bad;
+    }
+    return bad;
+}

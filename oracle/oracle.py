@@ -85,6 +85,11 @@ def lib():
                                     _opt(_i32p), _opt(_i32p), _opt(_f64p), i32,
                                     C.POINTER(i32)]
         L.orc_newton_ex.restype = i32
+        L.orc_sl3_retraction.argtypes = [_f64p, _f64p]
+        L.orc_nh_response.argtypes = [_f64p, f64, f64, f64, _f64p]
+        L.orc_element_states.argtypes = [u32, u32, _f64p, _u32p, _f64p, _f64p, _f64p, _f64p,
+                                         _f64p]
+        L.orc_element_states.restype = u32
         L.orc_exact_apply.argtypes = [u32, u32, _f64p, _u32p, _opt(_u8p), _f64p, _f64p,
                                       _f64p, _f64p, _f64p, i32]
         L.orc_param_grads.argtypes = [u32, _f64p, _u32p, _opt(_u8p), _f64p, _f64p, _f64p, _f64p]
@@ -130,6 +135,9 @@ def ref():
         R.ref_pcg_ilu0.argtypes = [u32, _u32p, _u32p, _f64p, _f64p, _f64p, f64, i32, i32]
         R.ref_pcg_ilu0.restype = i32
         R.ref_spmv.argtypes = [u32, _u32p, _u32p, _f64p, _f64p, _f64p]
+        if hasattr(R, "ref_sl3_retraction"):
+            R.ref_sl3_retraction.argtypes = [_f64p, _f64p]
+            R.ref_nh_response.argtypes = [_f64p, f64, f64, f64, _f64p]
         _ref = R
     return _ref
 
@@ -297,6 +305,30 @@ def newton_ex(xyz, conn, mu_e, lam_e, nu, rp, ci, slot, mask, bc_value, n_steps,
                              line_search, ls_c, diverge_rate, diverge_count, diverge_growth, u,
                              nps, pps, al, alpha_cap, C.byref(na))
     return u, st, nps, pps, al[:min(na.value, alpha_cap)]
+
+
+def sl3_retraction(G):
+    out = np.zeros(9)
+    lib().orc_sl3_retraction(np.ascontiguousarray(G, np.float64), out)
+    return out
+
+
+def nh_response(F, mu, lam, J):
+    sig = np.zeros(6)
+    lib().orc_nh_response(np.ascontiguousarray(F, np.float64), mu, lam, J, sig)
+    return sig
+
+
+def element_states(xyz, conn, mu_e, lam_e, u, F0=None, stress0=None):
+    """orc_element_states: (F_sl3 [E, 9], stress [E, 6], det violations);
+    untouched tets keep F0/stress0 (default identity / zero)"""
+    ne = conn.size // 4
+    F = (np.tile(np.eye(3).reshape(9), ne) if F0 is None else np.array(F0, np.float64)).ravel()
+    S = np.zeros(6 * ne) if stress0 is None else np.array(stress0, np.float64).ravel()
+    v = lib().orc_element_states(xyz.size // 3, ne, xyz, conn,
+                                 np.ascontiguousarray(mu_e, np.float64),
+                                 np.ascontiguousarray(lam_e, np.float64), u, F, S)
+    return F.reshape(ne, 9), S.reshape(ne, 6), int(v)
 
 
 def exact_apply(xyz, conn, mu_e, lam_e, u, v, transpose=False, active=None):

@@ -220,4 +220,18 @@ void ref_spmv(uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx, cons
     A.matvec(x, y);
 }
 
+// sl3_retraction(G, 0) (CORE/lie_operator.cpp:300) on a Matrix3x3 whose
+// data array is G9
+void ref_sl3_retraction(const double* G9, double* out9) {
+    atlas::Matrix3x3 G;
+    for (int i = 0; i < 9; ++i) G.data[i] = G9[i];
+    const atlas::Matrix3x3 R = atlas::sl3_retraction(G, atlas::Matrix3x3::zero());
+    for (int i = 0; i < 9; ++i) out9[i] = R.data[i];
+}
+
+// neo_hookean_response (:79) with the J given
+void ref_nh_response(const double* F9, double E, double nu, double J, double* sig6) {
+    neo_hookean_response(F9, E, nu, sig6, J);
+}
+
 }  // extern "C"

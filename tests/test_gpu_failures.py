@@ -165,3 +165,22 @@ def test_vanishing_pivot_is_perturbed_as_the_reference(fm):
         Lr, Ur, dr = np.zeros(ci.size), np.zeros(ci.size), np.zeros(3)
         R.ref_ilu0(3, rp, ci, val, Lr, Ur, dr, None)
         np.testing.assert_array_equal(d, dr)
+
+
+def test_flattened_element_takes_the_reference_guarded_inverse(fm):
+    """A tet deformed flat (det F ~ 1e-16, det C below 1e-30): the reference's
+    matrix_3x3_inv returns 1e30 I for C^-1 (FEM/adaptive_fem_engine.hpp:56-60)
+    and the stress becomes (mu (1 - 1e30) + lam ln(0.01) 1e30) C; the
+    element kernel reproduces it (oracle pinned to the reference)"""
+    x = np.array([0.0, 0.0, 0.0, 1.0, 0.1, 0.0, 0.2, 1.0, 0.1, 0.1, 0.3, 1.0])
+    y = x.copy()
+    y[2::3] = 0.0  # every vertex moved into the plane z = 0
+    u = y - x
+    E, nu = 1.0, 0.3
+    ctx = fm.Context(0)
+    K, f = ctx.elements(cu(x.reshape(1, 12)), cu(u.reshape(1, 12)), cu(np.array([E])), nu)
+    Ko, fo = O.element(x, u, E, nu)
+    K, f = K.cpu().numpy().ravel(), f.cpu().numpy().ravel()
+    assert np.abs(fo).max() > 1e20  # the guarded branch was taken
+    assert np.abs(f - fo).max() <= 1e-12 * np.abs(fo).max()
+    assert np.abs(K - Ko).max() <= 1e-12 * np.abs(Ko).max()

@@ -1,0 +1,66 @@
+"""Element state update on the GPU (fm_element_states, the device form of
+update_element_states_rigorous) against the oracle's restatement, which is
+pinned bit for bit to the reference's sl3_retraction and
+neo_hookean_response (tests/test_oracle_states.py).
+
+Tolerances: F_sl3 entries within 1e-12 absolute (they are O(1)); stresses
+within 1e-11 normwise relative (matrix log/exp chains of ~100 FP64
+operations, FMA-contracted on the GPU); the det-violation count exact."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def fm():
+    import flexmesh_b200 as F
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return F
+
+
+def block(fm, N=6):
+    from flexmesh_b200 import configs
+
+    P = configs.scaleup_block(N)
+    ctx = fm.Context(0)
+    ctx.set_mesh(P.xyz, P.conn, P.elem_volume)
+    ctx.set_material(P.E, P.nu, P.E_elem)
+    ctx.set_bc(P.mask, P.bc_value)
+    return ctx, P
+
+
+@pytest.mark.parametrize("amp", [1e-9, 0.02, 0.15])
+def test_element_states_match_oracle(fm, amp):
+    ctx, P = block(fm)
+    rng = np.random.default_rng(3)
+    u = amp * rng.standard_normal(P.xyz.size)
+    F, S, v = ctx.element_states(torch.as_tensor(u, device="cuda"))
+    mu, lam = P.lame()
+    Fo, So, vo = O.element_states(P.xyz, P.conn, mu, lam, u)
+    F, S = F.cpu().numpy(), S.cpu().numpy()
+    assert np.abs(F - Fo).max() <= 1e-12
+    assert np.abs(S - So).max() <= 1e-11 * max(np.abs(So).max(), 1e-300)
+    assert v == vo
+
+
+def test_states_follow_newton_iterations(fm):
+    """attached to a Newton load step, the states are those of the final u"""
+    ctx, P = block(fm)
+    ne = P.n_elems
+    F = torch.eye(3, dtype=torch.float64, device="cuda").reshape(1, 9).repeat(ne, 1).contiguous()
+    S = torch.zeros(ne, 6, dtype=torch.float64, device="cuda")
+    ctx.set_state_output(F, S)
+    u = torch.zeros(P.xyz.size, dtype=torch.float64, device="cuda")
+    r = ctx.newton_step_cfg(u, 1.0 / P.n_steps, inner_tol=1e-12)
+    assert r["status"] == 0
+    prof = ctx.profile_read()
+    assert prof["states"]["calls"] == r["newton_iters"]  # one update per update of u
+    ctx.set_state_output(None, None)
+    F2, S2, _ = ctx.element_states(u)
+    assert torch.equal(F, F2) and torch.equal(S, S2)
