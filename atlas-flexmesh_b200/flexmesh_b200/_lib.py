@@ -32,7 +32,8 @@ EXPORTS = [
     "fm_exact_apply", "fm_adjoint", "fm_csr_ilu0", "fm_newton_step", "fm_newton_step_host",
     "fm_profile_enable", "fm_profile_read", "fm_newton_config_default", "fm_newton_step_cfg",
     "fm_newton_history", "fm_set_wait_limit", "fm_check_wait", "fm_newton_step_cfg_host",
-    "fm_newton_solve_cfg", "fm_element_states", "fm_set_state_output",
+    "fm_newton_solve_cfg", "fm_element_states", "fm_set_state_output", "fm_checkpoint_save",
+    "fm_checkpoint_header", "fm_checkpoint_load",
 ]
 PROF_KINDS = {0: "assemble", 1: "ilu0", 2: "trsv", 3: "spmv", 4: "vector", 5: "states"}
 
@@ -61,6 +62,63 @@ class NewtonRecord(C.Structure):
     _fields_ = [("kind", C.c_int), ("pcg_iters", C.c_int), ("rnorm", C.c_double),
                 ("alpha", C.c_double), ("inner_tol", C.c_double), ("flags", C.c_uint32),
                 ("pad", C.c_uint32)]
+
+
+class Checkpoint(C.Structure):
+    """fm_checkpoint (include/fm_api.h): the reference's CheckpointFile layout"""
+    _fields_ = [("load_step", C.c_uint32), ("adapt_iter", C.c_uint32), ("n_nodes", C.c_uint32),
+                ("n_elems", C.c_uint32), ("n_dofs", C.c_uint32)] + [
+        (name, C.c_void_p) for name in ("xyz", "node_disp", "conn", "volume", "jacobian_det",
+                                         "quality", "F", "stress", "eps_plastic", "kappa",
+                                         "gamma_p", "u")]
+
+
+# checkpoint arrays: (name, dtype, entries per node / element / DOF)
+_CK_ARRAYS = [("xyz", np.float64, "n", 3), ("node_disp", np.float64, "n", 3),
+              ("conn", np.uint32, "e", 4), ("volume", np.float64, "e", 1),
+              ("jacobian_det", np.float64, "e", 1), ("quality", np.float64, "e", 1),
+              ("F", np.float64, "e", 9), ("stress", np.float64, "e", 6),
+              ("eps_plastic", np.float64, "e", 6), ("kappa", np.float64, "e", 1),
+              ("gamma_p", np.float64, "e", 1), ("u", np.float64, "d", 1)]
+
+
+def save_checkpoint(path, xyz, conn, u, load_step=0, adapt_iter=0, **arrays):
+    """fm_checkpoint_save: a restart file in the reference's CheckpointFile
+    layout; arrays: node_disp, volume, jacobian_det, quality, F, stress,
+    eps_plastic, kappa, gamma_p (host arrays; missing ones take the
+    ElementState defaults / zeros)"""
+    ck = Checkpoint()
+    keep = {"xyz": np.ascontiguousarray(xyz, np.float64),
+            "conn": np.ascontiguousarray(conn, np.uint32),
+            "u": np.ascontiguousarray(u, np.float64)}
+    for name, dt, _, _ in _CK_ARRAYS:
+        if name in arrays and arrays[name] is not None:
+            keep[name] = np.ascontiguousarray(arrays[name], dt)
+    ck.load_step, ck.adapt_iter = load_step, adapt_iter
+    ck.n_nodes, ck.n_elems, ck.n_dofs = keep["xyz"].size // 3, keep["conn"].size // 4, keep["u"].size
+    for name, a in keep.items():
+        setattr(ck, name, a.ctypes.data)
+    st = lib().fm_checkpoint_save(os.fsencode(path), C.byref(ck))
+    if st:
+        raise FMError(st, f"fm_checkpoint_save: cannot write {path}")
+
+
+def load_checkpoint(path):
+    """fm_checkpoint_load: every array of a CheckpointFile-layout file"""
+    ck = Checkpoint()
+    st = lib().fm_checkpoint_header(os.fsencode(path), C.byref(ck))
+    if st:
+        raise FMError(st, f"fm_checkpoint_header: cannot read {path}")
+    sizes = {"n": ck.n_nodes, "e": ck.n_elems, "d": ck.n_dofs}
+    out = {}
+    for name, dt, kind, k in _CK_ARRAYS:
+        out[name] = np.zeros(sizes[kind] * k, dt)
+        setattr(ck, name, out[name].ctypes.data)
+    st = lib().fm_checkpoint_load(os.fsencode(path), C.byref(ck))
+    if st:
+        raise FMError(st, f"fm_checkpoint_load: cannot read {path}")
+    out["load_step"], out["adapt_iter"] = ck.load_step, ck.adapt_iter
+    return out
 
 
 class FMError(RuntimeError):
@@ -123,6 +181,9 @@ def lib() -> C.CDLL:
             "fm_newton_solve_cfg": [_vp, _vp, _i32, _i32, _P(NewtonConfig), _P(NewtonResult)],
             "fm_element_states": [_vp, _vp, _vp, _vp, _P(_u32)],
             "fm_set_state_output": [_vp, _vp, _vp],
+            "fm_checkpoint_save": [C.c_char_p, _P(Checkpoint)],
+            "fm_checkpoint_header": [C.c_char_p, _P(Checkpoint)],
+            "fm_checkpoint_load": [C.c_char_p, _P(Checkpoint)],
             "fm_set_wait_limit": [_vp, _u64],
             "fm_check_wait": [_vp],
             "fm_profile_enable": [_vp, _i32],

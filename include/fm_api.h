@@ -407,6 +407,39 @@ fm_status fm_element_states(fm_ctx* ctx, const double* u_dev, double* F_dev, dou
  * engine does after each Newton iteration (:2589).  NULL, NULL detaches. */
 fm_status fm_set_state_output(fm_ctx* ctx, double* F_dev, double* stress_dev);
 
+/* ---- restart files (host only) ---------------------------------------------
+ * Replaces CheckpointFile::save / load (FEM/adaptive_fem_engine.hpp:
+ * 1347-1452) with the same byte layout, so files interchange with the
+ * reference's: header u32 load_step, adapt_iter, n_nodes, n_elements, n_dofs;
+ * per node f64 x, y, z, u, v, w; per element u32 nodes[4], f64 volume,
+ * jacobian_det, quality_metric; per element state f64 F[9], stress[6],
+ * eps_plastic[6], kappa, gamma_p; then n_dofs f64 of the solution.
+ * Array pointers are host arrays of the sizes the counts give; on save a
+ * NULL array is written as ElementState::initialize / zero-filled values
+ * (xyz, conn and, when n_dofs > 0, u are required); on load a NULL array is
+ * skipped.  fm_checkpoint_header reads the five header words, so the
+ * caller can size its arrays; fm_checkpoint_load then needs the same
+ * counts in *ck.  I/O failures return FM_ERR_ARG. */
+typedef struct {
+    uint32_t load_step, adapt_iter;
+    uint32_t n_nodes, n_elems, n_dofs;
+    double* xyz;           /* 3 n_nodes: MeshNode x, y, z */
+    double* node_disp;     /* 3 n_nodes: MeshNode u, v, w */
+    uint32_t* conn;        /* 4 n_elems */
+    double* volume;        /* n_elems */
+    double* jacobian_det;  /* n_elems */
+    double* quality;       /* n_elems */
+    double* F;             /* 9 n_elems: ElementState::F_data */
+    double* stress;        /* 6 n_elems */
+    double* eps_plastic;   /* 6 n_elems */
+    double* kappa;         /* n_elems */
+    double* gamma_p;       /* n_elems */
+    double* u;             /* n_dofs */
+} fm_checkpoint;
+fm_status fm_checkpoint_save(const char* path, const fm_checkpoint* ck);
+fm_status fm_checkpoint_header(const char* path, fm_checkpoint* ck);
+fm_status fm_checkpoint_load(const char* path, fm_checkpoint* ck);
+
 /* ---- A9/A21: exact Jacobian and adjoint (no reference counterpart) --------
  * fm_exact_apply: y = K_exact v (transpose = 0) or K_exact^T v (1), the
  * derivative of the element forces f_int(u) at u (not the reference's

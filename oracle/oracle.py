@@ -135,6 +135,13 @@ def ref():
         R.ref_pcg_ilu0.argtypes = [u32, _u32p, _u32p, _f64p, _f64p, _f64p, f64, i32, i32]
         R.ref_pcg_ilu0.restype = i32
         R.ref_spmv.argtypes = [u32, _u32p, _u32p, _f64p, _f64p, _f64p]
+        if hasattr(R, "ref_checkpoint_save"):
+            R.ref_checkpoint_save.argtypes = [C.c_char_p, i32, _f64p, _opt(_f64p), _opt(_f64p),
+                                              u32, u32]
+            R.ref_checkpoint_save.restype = i32
+            R.ref_checkpoint_load.argtypes = [C.c_char_p] + [C.POINTER(u32)] * 5 + [
+                _opt(_f64p), _opt(_f64p), _opt(_f64p), u32, u32]
+            R.ref_checkpoint_load.restype = i32
         if hasattr(R, "ref_sl3_retraction"):
             R.ref_sl3_retraction.argtypes = [_f64p, _f64p]
             R.ref_nh_response.argtypes = [_f64p, f64, f64, f64, _f64p]

@@ -234,4 +234,42 @@ void ref_nh_response(const double* F9, double E, double nu, double J, double* si
     neo_hookean_response(F9, E, nu, sig6, J);
 }
 
+// CheckpointFile::save (:1350) of the reference's own unit cube N with the
+// given solution (also copied into MeshNode::u, v, w) and states F/stress
+// (nullable: the ElementState defaults)
+int ref_checkpoint_save(const char* path, int N, const double* u, const double* F,
+                        const double* stress, uint32_t load_step, uint32_t adapt_iter) {
+    MeshTopology mesh = generate_unit_cube_mesh(N);
+    std::vector<double> uu(u, u + mesh.n_dofs);
+    for (size_t n = 0; n < mesh.nodes.size(); ++n) {
+        mesh.nodes[n].u = u[3 * n];
+        mesh.nodes[n].v = u[3 * n + 1];
+        mesh.nodes[n].w = u[3 * n + 2];
+    }
+    for (size_t e = 0; e < mesh.states.size(); ++e) {
+        if (F) std::memcpy(mesh.states[e].F_data, F + 9 * e, sizeof(double) * 9);
+        if (stress) std::memcpy(mesh.states[e].stress, stress + 6 * e, sizeof(double) * 6);
+    }
+    return CheckpointFile::save(path, mesh, uu, load_step, adapt_iter) ? 0 : 1;
+}
+
+// CheckpointFile::load (:1402): sizes, the solution, and the states
+int ref_checkpoint_load(const char* path, uint32_t* n_nodes, uint32_t* n_elems, uint32_t* n_dofs,
+                        uint32_t* load_step, uint32_t* adapt_iter, double* u_out, double* F_out,
+                        double* stress_out, uint32_t cap_dofs, uint32_t cap_elems) {
+    MeshTopology mesh;
+    std::vector<double> u;
+    if (!CheckpointFile::load(path, mesh, u, *load_step, *adapt_iter)) return 1;
+    *n_nodes = (uint32_t)mesh.nodes.size();
+    *n_elems = (uint32_t)mesh.elements.size();
+    *n_dofs = mesh.n_dofs;
+    if (u.size() <= cap_dofs && u_out) std::memcpy(u_out, u.data(), sizeof(double) * u.size());
+    if (mesh.states.size() <= cap_elems)
+        for (size_t e = 0; e < mesh.states.size(); ++e) {
+            if (F_out) std::memcpy(F_out + 9 * e, mesh.states[e].F_data, sizeof(double) * 9);
+            if (stress_out) std::memcpy(stress_out + 6 * e, mesh.states[e].stress, sizeof(double) * 6);
+        }
+    return 0;
+}
+
 }  // extern "C"
