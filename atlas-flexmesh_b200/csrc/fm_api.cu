@@ -1249,6 +1249,7 @@ fm_status fm_newton_config_default(fm_newton_config* g) {
     g->diverge_count = 3;
     g->diverge_growth = 10.0;
     g->precision = FM_FP64;
+    g->ilu_every = 1;
     return FM_OK;
 }
 
@@ -1257,7 +1258,7 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
     if (res) std::memset(res, 0, sizeof *res);
     TRY(need_material(c));
     if (!u || !g || g->max_newton < 1 || g->line_search < 0 || g->max_pcg < 1 ||
-        !(g->inner_tol > 0.0))
+        !(g->inner_tol > 0.0) || g->ilu_every < 1)
         return fail(c, FM_ERR_ARG, "bad argument");
     const int prec = g->precision;
     if (prec != FM_FP64 && prec != FM_MIXED) return fail(c, FM_ERR_ARG, "unknown precision");
@@ -1283,10 +1284,12 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
 
     // ILU(0) of the eliminated tangent, PCG on R (norm rnorm) to itol, then
     // either u += du or du kept in `du` (FP64) for the line search.
+    int n_solve = 0;
     auto solve = [&](double rnorm, double itol, bool keep, int* its) -> fm_status {
+        const bool refactor = n_solve++ % g->ilu_every == 0;
         if (mixed) {
             // FP32 tangent/ILU(0)/PCG on R/||R||; the step is rescaled in FP64
-            TRY(ilu_core<float>(c, c->fem, c->w32.K.p, c->w32.LU.p, c->w32.diag.p));
+            if (refactor) TRY(ilu_core<float>(c, c->fem, c->w32.K.p, c->w32.LU.p, c->w32.diag.p));
             { PROF(FM_PROF_VECTOR, 1); fm::launch_to_f32_scaled(c->n, R, 1.0 / rnorm, c->w32.b.p, c->w32.x.p, c->stream); }
             Op<float> A{c, &c->fem, true, c->w32.K.p, c->w32.LU.p, c->w32.diag.p, c->w32.t.p,
                         c->grid_trsv32, c->w32.dinv.p};
@@ -1295,7 +1298,7 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
             if (keep) { PROF(FM_PROF_VECTOR, 1); fm::launch_f32_to_f64_scaled(c->n, c->w32.x.p, rnorm, du, c->stream); }
             else { PROF(FM_PROF_VECTOR, 1); fm::launch_axpy_u_f32(c->n, c->w32.x.p, rnorm, u, c->stream); }
         } else {
-            TRY(ilu_core<double>(c, c->fem, c->w64.K.p, c->w64.LU.p, c->w64.diag.p));
+            if (refactor) TRY(ilu_core<double>(c, c->fem, c->w64.K.p, c->w64.LU.p, c->w64.diag.p));
             CK(cudaMemsetAsync(du, 0, sizeof(double) * c->n, c->stream));
             Op<double> A{c, &c->fem, true, c->w64.K.p, c->w64.LU.p, c->w64.diag.p, c->w64.t.p,
                          c->grid_trsv64, c->w64.dinv.p};

@@ -42,11 +42,15 @@ METRIC = "Newton solve s & tets/s, 1.57M-tet block: mixed vs FP64 GPU at rel err
 WORKLOAD = "scale-up block 64^3x6 tets (1,572,864 tets, 823,875 DOF), jitter 0.15h, " \
            "log-normal mu sigma 0.3, top u_z=-0.2 in 10 load steps"
 
-# Newton settings of the mixed path (fm_newton_config fields)
+# Newton settings of the mixed path (fm_newton_config fields).  Both paths
+# run the engine's Armijo line search on every iteration (10 trials,
+# c = 1e-4, FEM/adaptive_fem_engine.hpp:2581): without it the reference's
+# tangent stops contracting at load levels 8-10 of this block.
 MIXED = dict(newton_rtol=1e-10, inner_tol=0.2, predictor_tol=1e-6, max_newton=400,
-             max_pcg=20000)
-# the plain FP64 path: PCG to 1e-12 as the reference's Newton loop asks
-FP64 = dict(newton_rtol=1e-10, inner_tol=1e-12, max_newton=400, max_pcg=20000)
+             max_pcg=20000, line_search=10, ls_c=1e-4)
+# the plain FP64 path: PCG to 1e-12
+FP64 = dict(newton_rtol=1e-10, inner_tol=1e-12, max_newton=400, max_pcg=20000, line_search=10,
+            ls_c=1e-4)
 
 
 def parse():

@@ -308,7 +308,7 @@ fm_status fm_newton_step_host(fm_ctx* ctx, double* u_host, double load_frac, dou
  * inner_tol 1e-12, predictor_tol 0 (= inner_tol), inner_tol_min 0 (off),
  * max_newton 200, max_pcg 5000, line_search 10 with ls_c 1e-4 (the engine's
  * armijo_line_search_true(..., line_search_c = 1e-4, 10), :2314, :2581),
- * diverge_rate 0 (off), diverge_count 3, diverge_growth 10, FP64. */
+ * diverge_rate 0 (off), diverge_count 3, diverge_growth 10, FP64, ilu_every 1. */
 typedef struct {
     double newton_rtol;    /* stop when ||R|| < newton_rtol ||R_0|| */
     double newton_atol;    /* ... or ||R|| < newton_atol */
@@ -323,6 +323,10 @@ typedef struct {
     int diverge_count;     /* slow iterations tolerated (reference 3) */
     double diverge_growth; /* growth factor that stops at once (reference 10; <= 0: off) */
     int precision;         /* fm_precision */
+    int ilu_every;         /* refactorize the ILU(0) preconditioner at every ilu_every-th
+                              solve of a load step (1: every solve, as pcg_solve_ilu0
+                              does; k > 1: an earlier tangent's factors precondition
+                              the current tangent, which PCG still solves) */
 } fm_newton_config;
 
 typedef struct {
