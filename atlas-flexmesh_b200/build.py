@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "flexmesh_b200", "libflexmesh_b200.so")
-SOURCES = ["fm_api.cu", "fm_kernels.cu", "fm_nodes.cu", "fm_trsv.cu", "fm_trsv_push.cu", "fm_adjoint.cu", "fm_states.cu",
+SOURCES = ["fm_api.cu", "fm_kernels.cu", "fm_nodes.cu", "fm_trsv.cu", "fm_trsv_push.cu", "fm_adjoint.cu", "fm_states.cu", "fm_meshsetup.cu",
            "fm_setup.cpp", "fm_checkpoint.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

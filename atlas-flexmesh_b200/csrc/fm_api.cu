@@ -16,40 +16,16 @@
 #include <vector>
 
 #include "fm_api.h"
+#include "fm_devbuf.hpp"
 #include "fm_kernels.hpp"
 #include "fm_adjoint.hpp"
+#include "fm_meshsetup.hpp"
 #include "fm_nodes.hpp"
 #include "fm_setup.hpp"
 
 namespace {
 
-template <typename T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    ~DevBuf() { release(); }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    // (re)allocate to at least count elements; contents undefined
-    cudaError_t reserve(size_t count) {
-        if (count <= n && p) return cudaSuccess;
-        release();
-        if (count == 0) return cudaSuccess;
-        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return e;
-        }
-        n = count;
-        return cudaSuccess;
-    }
-};
+using fm::DevBuf;
 
 struct SolverCsr {
     uint32_t n = 0;
@@ -92,7 +68,7 @@ struct fm_ctx {
     std::vector<uint32_t> h_conn;
     std::vector<uint8_t> h_skip;
     fm::NodeGraph graph;
-    fm::Incidence inc;
+    std::vector<uint32_t> node_lp, node_lo, node_up, node_uo;  // node levels (ptr, order)
     DevBuf<double> xyz;
     DevBuf<uint4> conn;
     DevBuf<uint32_t> nbr_ptr, nbr, inc_ptr, inc_e;
@@ -319,7 +295,7 @@ fm::MeshDev mesh_view(const fm_ctx* c) {
 // pointers, columns, first-diagonal/first-upper positions and the DOF-level
 // dependency orders that the sync-free kernels walk.
 fm_status setup_solver_csr(fm_ctx* c, SolverCsr& S, uint32_t n, std::vector<uint32_t>&& rp,
-                           std::vector<uint32_t>&& ci, bool keep_levels) {
+                           std::vector<uint32_t>&& ci) {
     S.n = n;
     S.nnz = rp[n];
     std::vector<uint32_t> dpos(n), upos(n);
@@ -342,12 +318,6 @@ fm_status setup_solver_csr(fm_ctx* c, SolverCsr& S, uint32_t n, std::vector<uint
     CK(upload(S.upos, upos.data(), n, c->stream));
     CK(upload(S.fwd, fr.data(), fr.size(), c->stream));
     CK(upload(S.bwd, br.data(), br.size(), c->stream));
-    if (keep_levels) {
-        c->lvl_fwd_ptr = std::move(fp);
-        c->lvl_fwd_rows = std::move(fr);
-        c->lvl_bwd_ptr = std::move(bp);
-        c->lvl_bwd_rows = std::move(br);
-    }
     S.h_rp = std::move(rp);
     S.h_ci = std::move(ci);
     CK(c->done.reserve(std::max<size_t>(c->done.n, n + 1)));
@@ -623,6 +593,64 @@ fm_status ensure_matrix(fm_ctx* c) {
     return ensure_vectors<T>(c, c->n);
 }
 
+// DOF-level dependency levels of the solve pattern from the node levels:
+// node n's rows hold all three DOFs of n and of each neighbour, so row 3n+d
+// sits at depth 3 D(n) + d below and 3 D_U(n) + 2 - d above (D: node depth),
+// and at depth 0 in both directions when n has no entries at all.  Rows of a
+// level ascend, as a stable sort by depth orders them.
+fm_status ensure_dof_levels(fm_ctx* c) {
+    if (!c->lvl_fwd_ptr.empty() && !c->lvl_bwd_ptr.empty()) return FM_OK;
+    const uint32_t nn = c->nn, n = c->n;
+    for (int lower = 1; lower >= 0; --lower) {
+        const std::vector<uint32_t>& lp = lower ? c->node_lp : c->node_up;
+        const std::vector<uint32_t>& lo = lower ? c->node_lo : c->node_uo;
+        std::vector<uint32_t> depth(n, 0);
+        uint32_t maxd = 0;
+        for (size_t l = 0; l + 1 < lp.size(); ++l)
+            for (uint32_t t = lp[l]; t < lp[l + 1]; ++t) {
+                const uint32_t nd = lo[t];
+                if (c->graph.ptr[nd + 1] == c->graph.ptr[nd]) continue;  // no entries
+                for (uint32_t d = 0; d < 3; ++d) {
+                    const uint32_t dep = 3 * (uint32_t)l + (lower ? d : 2 - d);
+                    depth[3 * nd + d] = dep;
+                    maxd = std::max(maxd, dep);
+                }
+            }
+        std::vector<uint32_t>& ptr = lower ? c->lvl_fwd_ptr : c->lvl_bwd_ptr;
+        std::vector<uint32_t>& rows = lower ? c->lvl_fwd_rows : c->lvl_bwd_rows;
+        const uint32_t nl = n ? maxd + 1 : 0;
+        ptr.assign(nl + 1, 0);
+        for (uint32_t i = 0; i < n; ++i) ptr[depth[i] + 1]++;
+        for (uint32_t l = 0; l < nl; ++l) ptr[l + 1] += ptr[l];
+        rows.resize(n);
+        std::vector<uint32_t> fill(ptr.begin(), ptr.end() - (nl ? 1 : 0));
+        for (uint32_t i = 0; i < n; ++i) rows[fill[depth[i]]++] = i;
+    }
+    (void)nn;
+    return FM_OK;
+}
+
+// element -> CSR slot maps on the device (chunks of 2^20 tets through a
+// scratch buffer): into host memory, or into a device buffer
+fm_status slot_map_device(fm_ctx* c, int reference, int32_t* host_out, DevBuf<int32_t>* dev_out) {
+    const uint32_t chunk = 1u << 20;
+    DevBuf<int32_t> tmp;
+    if (dev_out) CK(dev_out->reserve(144 * (size_t)std::max(c->ne, 1u)));
+    else CK(tmp.reserve(144 * (size_t)std::min(c->ne, chunk)));
+    for (uint32_t e0 = 0; e0 < c->ne; e0 += chunk) {
+        const uint32_t cnt = std::min(chunk, c->ne - e0);
+        int32_t* dst = dev_out ? dev_out->p + 144 * (size_t)e0 : tmp.p;
+        fm::launch_slot_map(e0, cnt, c->conn.p, c->nbr_ptr.p, c->nbr.p, reference, dst,
+                            c->stream);
+        CK(cudaGetLastError());
+        if (host_out)
+            CK(cudaMemcpyAsync(host_out + 144 * (size_t)e0, dst, 144 * sizeof(int32_t) * cnt,
+                               cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return FM_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -730,6 +758,19 @@ fm_status fm_sizes(const fm_ctx* c, uint32_t* n_nodes, uint32_t* n_elems, uint32
     return FM_OK;
 }
 
+fm_status fm_mesh_coloring(uint32_t n_nodes, uint32_t n_elems, const uint32_t* conn,
+                           uint32_t* colors, uint32_t* n_colors) {
+    if (!conn || !colors || !n_colors) return FM_ERR_ARG;
+    for (size_t q = 0; q < 4 * (size_t)n_elems; ++q)
+        if (conn[q] >= n_nodes) return FM_ERR_ARG;
+    try {
+        *n_colors = fm::mesh_coloring(n_nodes, n_elems, conn, colors);
+    } catch (const std::bad_alloc&) {
+        return FM_ERR_OOM;
+    }
+    return FM_OK;
+}
+
 fm_status fm_unit_cube_sizes(int N, uint32_t* n_nodes, uint32_t* n_elems) {
     if (N < 1 || N > 1200 || !n_nodes || !n_elems) return FM_ERR_ARG;
     const uint64_t s = (uint64_t)N + 1;
@@ -751,6 +792,9 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
     if (n_nodes >= (1u << 30)) return fail(c, FM_ERR_ARG, "n_nodes too large");
     try {
         CK(cudaSetDevice(c->device));
+        // a new mesh starts with clear flags (a stale timeout would stop the
+        // level pass's waits at once)
+        CK(cudaMemsetAsync(&c->sc.p->status, 0, sizeof(unsigned), c->stream));
         for (size_t q = 0; q < 4 * (size_t)n_elems; ++q)
             if (conn[q] >= n_nodes)
                 return fail(c, FM_ERR_ARG, "conn[%zu] = %u out of range", q, conn[q]);
@@ -762,17 +806,6 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
         c->h_skip.assign(n_elems, 0);
         if (elem_volume)
             for (uint32_t e = 0; e < n_elems; ++e) c->h_skip[e] = !(elem_volume[e] >= 1e-30);
-        c->graph = fm::build_node_graph(n_nodes, n_elems, conn);
-        c->inc = fm::build_incidence(n_nodes, n_elems, conn);
-        if (c->graph.max_deg > 32 || c->inc.max_inc > 32)
-            return fail(c, FM_ERR_LIMITS,
-                        "mesh valence beyond kernel limits (max neighbours %u, max incident "
-                        "tets %u; both must be <= 32)",
-                        c->graph.max_deg, c->inc.max_inc);
-        const uint64_t nnz = 9ull * c->graph.ptr[n_nodes];
-        if (nnz >= (1ull << 32)) return fail(c, FM_ERR_LIMITS, "nnz %llu exceeds 32-bit CSR",
-                                             (unsigned long long)nnz);
-        c->nnz = nnz;
         std::vector<uint4> cw(n_elems);
         for (uint32_t e = 0; e < n_elems; ++e) {
             const uint32_t* q = conn + 4 * (size_t)e;
@@ -780,43 +813,51 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
         }
         CK(upload(c->xyz, xyz, 3 * (size_t)n_nodes, c->stream));
         CK(upload(c->conn, cw.data(), n_elems, c->stream));
-        CK(upload(c->nbr_ptr, c->graph.ptr.data(), c->graph.ptr.size(), c->stream));
-        CK(upload(c->nbr, c->graph.nbr.data(), c->graph.nbr.size(), c->stream));
-        CK(upload(c->inc_ptr, c->inc.ptr.data(), c->inc.ptr.size(), c->stream));
-        CK(upload(c->inc_e, c->inc.elem.data(), c->inc.elem.size(), c->stream));
-        std::vector<uint32_t> rp(c->n + 1), ci(nnz);
-        fm::csr_row_ptr(c->graph, rp.data());
-        fm::csr_solve_cols(c->graph, ci.data());
-        TRY(setup_solver_csr(c, c->fem, c->n, std::move(rp), std::move(ci), true));
-        {
-            std::vector<uint32_t> lp, lo, up, uo;
-            c->node_levels_fwd = fm::node_levels(c->graph, true, lp, lo);
-            c->node_levels_bwd = fm::node_levels(c->graph, false, up, uo);
-            c->width_fwd = c->width_bwd = 0;
-            for (size_t l = 0; l + 1 < lp.size(); ++l)
-                c->width_fwd = std::max(c->width_fwd, lp[l + 1] - lp[l]);
-            for (size_t l = 0; l + 1 < up.size(); ++l)
-                c->width_bwd = std::max(c->width_bwd, up[l + 1] - up[l]);
-            CK(upload(c->self_pos, c->graph.self.data(), c->graph.self.size(), c->stream));
-            {
-                std::vector<uint32_t> ep;
-                std::vector<uint8_t> em;
-                fm::ilu_edge_maps(c->graph, ep, em);
-                CK(upload(c->emap_ptr, ep.data(), ep.size(), c->stream));
-                CK(upload(c->emap, em.data(), em.size(), c->stream));
-            }
-            CK(upload(c->node_fwd, lo.data(), lo.size(), c->stream));
-            CK(upload(c->node_bwd, uo.data(), uo.size(), c->stream));
-            // one 16-byte schedule record per position of each order
-            const std::vector<uint4> rf = node_records(c->graph, lo);
-            const std::vector<uint4> rb = node_records(c->graph, uo);
-            CK(upload(c->node_fwd_rec, rf.data(), rf.size(), c->stream));
-            CK(upload(c->node_bwd_rec, rb.data(), rb.size(), c->stream));
-            TRY(setup_push_solves(c, lp, lo, up, uo));
-            CK(cudaStreamSynchronize(c->stream));
-            CK(c->done.reserve(std::max<size_t>(c->done.n, (size_t)c->nn + 1)));
-            CK(cudaMemsetAsync(c->done.p, 0, c->done.n * sizeof(unsigned), c->stream));
-        }
+        // incidence, node graph, dependency levels, ILU maps and the
+        // assembly's scatter structure, built on the device
+        fm::MeshSetupDev md{&c->inc_ptr,      &c->inc_e,    &c->nbr_ptr,  &c->nbr,
+                            &c->self_pos,     &c->node_fwd, &c->node_bwd, &c->node_fwd_rec,
+                            &c->node_bwd_rec, &c->emap_ptr, &c->emap,     &c->inc_pos,
+                            &c->nbr_members};
+        fm::MeshSetupHost mh;
+        int res = fm::kSetupOk;
+        CK(fm::build_mesh_device(n_nodes, n_elems, c->conn.p, md, mh, c->status(), &res,
+                                 c->stream));
+        if (res == fm::kSetupTimeout)
+            return fail(c, FM_ERR_TIMEOUT, "fm_set_mesh: a bounded wait of the level pass expired");
+        if (res == fm::kSetupLimits)
+            return fail(c, FM_ERR_LIMITS,
+                        "mesh valence beyond kernel limits (max neighbours %u, max incident "
+                        "tets %u; both must be <= 32)",
+                        mh.graph.max_deg, mh.max_inc);
+        c->graph = std::move(mh.graph);
+        const uint64_t nnz = 9ull * c->graph.ptr[n_nodes];
+        if (nnz >= (1ull << 32)) return fail(c, FM_ERR_LIMITS, "nnz %llu exceeds 32-bit CSR",
+                                             (unsigned long long)nnz);
+        c->nnz = nnz;
+        // the scalar CSR and its DOF-level levels are built on first use
+        // (fm_build_pattern, fm_levels): the node kernels never read them
+        c->fem.n = c->n;
+        c->fem.nnz = nnz;
+        c->fem.h_rp.clear();
+        c->fem.h_ci.clear();
+        c->lvl_fwd_ptr.clear();
+        c->lvl_bwd_ptr.clear();
+        c->node_lp = std::move(mh.lp);
+        c->node_lo = std::move(mh.lo);
+        c->node_up = std::move(mh.up);
+        c->node_uo = std::move(mh.uo);
+        c->node_levels_fwd = (uint32_t)c->node_lp.size() - 1;
+        c->node_levels_bwd = (uint32_t)c->node_up.size() - 1;
+        c->width_fwd = c->width_bwd = 0;
+        for (size_t l = 0; l + 1 < c->node_lp.size(); ++l)
+            c->width_fwd = std::max(c->width_fwd, c->node_lp[l + 1] - c->node_lp[l]);
+        for (size_t l = 0; l + 1 < c->node_up.size(); ++l)
+            c->width_bwd = std::max(c->width_bwd, c->node_up[l + 1] - c->node_up[l]);
+        TRY(setup_push_solves(c, c->node_lp, c->node_lo, c->node_up, c->node_uo));
+        CK(cudaStreamSynchronize(c->stream));
+        CK(c->done.reserve(std::max<size_t>(c->done.n, (size_t)c->nn + 1)));
+        CK(cudaMemsetAsync(c->done.p, 0, c->done.n * sizeof(unsigned), c->stream));
         c->w64.factor_valid = c->w32.factor_valid = false;
         c->has_bc = false;
         c->has_mat = false;
@@ -824,32 +865,6 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
         CK(c->vec_a.reserve(c->n));
         CK(c->vec_b.reserve(c->n));
         CK(c->elem_rec.reserve(std::max<size_t>(1, (size_t)c->ne * fm::kElemRecBytes)));
-        {
-            // node-pass scatter structure: for every (node, incident tet) the
-            // tet's vertex positions in the node's neighbour list, and for
-            // every (node, neighbour) the incident tets on that edge
-            std::vector<uint32_t> ipos(c->inc.elem.size(), 0xffffffffu);
-            std::vector<uint32_t> memb(c->graph.nbr.size(), 0u);
-            for (uint32_t nd = 0; nd < c->nn; ++nd) {
-                const uint32_t* nl = c->graph.nbr.data() + c->graph.ptr[nd];
-                const uint32_t deg = c->graph.ptr[nd + 1] - c->graph.ptr[nd];
-                for (uint32_t i = c->inc.ptr[nd]; i < c->inc.ptr[nd + 1]; ++i) {
-                    const uint32_t e = c->inc.elem[i], l = i - c->inc.ptr[nd];
-                    uint32_t pk = 0;
-                    for (int q = 0; q < 4; ++q) {
-                        const uint32_t v = conn[4 * (size_t)e + q];
-                        const uint32_t* hit = std::lower_bound(nl, nl + deg, v);
-                        const uint32_t p = (hit != nl + deg && *hit == v) ? (uint32_t)(hit - nl) : 0xffu;
-                        pk |= p << (8 * q);
-                        if (p != 0xffu && v != nd && !c->h_skip[e])
-                            memb[c->graph.ptr[nd] + p] |= 1u << l;
-                    }
-                    ipos[i] = pk;
-                }
-            }
-            CK(upload(c->inc_pos, ipos.data(), ipos.size(), c->stream));
-            CK(upload(c->nbr_members, memb.data(), memb.size(), c->stream));
-        }
         CK(cudaStreamSynchronize(c->stream));
     } catch (const std::bad_alloc&) {
         return fail(c, FM_ERR_OOM, "host allocation failed in fm_set_mesh");
@@ -861,20 +876,18 @@ fm_status fm_build_pattern(fm_ctx* c, fm_pattern kind, uint32_t* row_ptr_out,
                            uint32_t* col_idx_out, int32_t* slot_map_out) {
     TRY(need_mesh(c));
     try {
-        std::vector<uint32_t> ref_cols;
-        const uint32_t* cols = c->fem.h_ci.data();
-        if (kind == FM_PATTERN_REFERENCE) {
-            ref_cols.resize(c->nnz);
-            fm::csr_reference_cols(c->graph, ref_cols.data());
-            cols = ref_cols.data();
-        } else if (kind != FM_PATTERN_SOLVE) {
+        if (kind != FM_PATTERN_REFERENCE && kind != FM_PATTERN_SOLVE)
             return fail(c, FM_ERR_ARG, "unknown pattern kind %d", (int)kind);
+        if (row_ptr_out) {
+            row_ptr_out[0] = 0;
+            fm::csr_row_ptr(c->graph, row_ptr_out);
         }
-        if (row_ptr_out)
-            std::memcpy(row_ptr_out, c->fem.h_rp.data(), sizeof(uint32_t) * (c->n + 1));
-        if (col_idx_out) std::memcpy(col_idx_out, cols, sizeof(uint32_t) * c->nnz);
+        if (col_idx_out) {
+            if (kind == FM_PATTERN_REFERENCE) fm::csr_reference_cols(c->graph, col_idx_out);
+            else fm::csr_solve_cols(c->graph, col_idx_out);
+        }
         if (slot_map_out)
-            fm::slot_map(c->fem.h_rp.data(), cols, c->ne, c->h_conn.data(), slot_map_out);
+            TRY(slot_map_device(c, kind == FM_PATTERN_REFERENCE, slot_map_out, nullptr));
     } catch (const std::bad_alloc&) {
         return fail(c, FM_ERR_OOM, "host allocation failed in fm_build_pattern");
     }
@@ -1002,17 +1015,7 @@ fm_status fm_residual(fm_ctx* c, const double* u, double* f) {
 fm_status fm_assemble_reference_pattern(fm_ctx* c, const double* u, double* K, double* f) {
     TRY(need_material(c));
     if (!u || !K || !f) return fail(c, FM_ERR_ARG, "null argument");
-    try {
-        if (!c->ref_slot.p) {
-            std::vector<uint32_t> cols(c->nnz);
-            fm::csr_reference_cols(c->graph, cols.data());
-            std::vector<int32_t> slot(144 * (size_t)c->ne);
-            fm::slot_map(c->fem.h_rp.data(), cols.data(), c->ne, c->h_conn.data(), slot.data());
-            CK(upload(c->ref_slot, slot.data(), slot.size(), c->stream));
-        }
-    } catch (const std::bad_alloc&) {
-        return fail(c, FM_ERR_OOM, "host allocation failed");
-    }
+    if (!c->ref_slot.p) TRY(slot_map_device(c, 1, nullptr, &c->ref_slot));
     CK(c->ke_scratch.reserve(144 * (size_t)c->ne));
     CK(cudaMemsetAsync(K, 0, sizeof(double) * c->nnz, c->stream));
     CK(cudaMemsetAsync(f, 0, sizeof(double) * c->n, c->stream));
@@ -1027,6 +1030,11 @@ fm_status fm_assemble_reference_pattern(fm_ctx* c, const double* u, double* K, d
 fm_status fm_levels(fm_ctx* c, uint32_t* fwd_ptr, uint32_t* fwd_rows, uint32_t* bwd_ptr,
                     uint32_t* bwd_rows, uint32_t* n_fwd, uint32_t* n_bwd) {
     TRY(need_mesh(c));
+    try {
+        TRY(ensure_dof_levels(c));
+    } catch (const std::bad_alloc&) {
+        return fail(c, FM_ERR_OOM, "host allocation failed in fm_levels");
+    }
     if (fwd_ptr) std::copy(c->lvl_fwd_ptr.begin(), c->lvl_fwd_ptr.end(), fwd_ptr);
     if (fwd_rows) std::copy(c->lvl_fwd_rows.begin(), c->lvl_fwd_rows.end(), fwd_rows);
     if (bwd_ptr) std::copy(c->lvl_bwd_ptr.begin(), c->lvl_bwd_ptr.end(), bwd_ptr);
@@ -1213,7 +1221,7 @@ fm_status fm_csr_pcg_ilu0(fm_ctx* c, uint32_t n, const uint32_t* row_ptr,
             }
         }
         if (c->gen.n != n || c->gen.h_rp != rp || c->gen.h_ci != ci)
-            TRY(setup_solver_csr(c, c->gen, n, std::move(rp), std::move(ci), false));
+            TRY(setup_solver_csr(c, c->gen, n, std::move(rp), std::move(ci)));
         CK(upload(c->gen_K, v.data(), nnz, c->stream));
         CK(c->gen_LU.reserve(nnz));
         CK(c->gen_diag.reserve(n));
@@ -1590,7 +1598,7 @@ fm_status fm_csr_ilu0(fm_ctx* c, uint32_t n, const uint32_t* row_ptr, const uint
             }
         }
         if (c->gen.n != n || c->gen.h_rp != rp || c->gen.h_ci != ci)
-            TRY(setup_solver_csr(c, c->gen, n, std::move(rp), std::move(ci), false));
+            TRY(setup_solver_csr(c, c->gen, n, std::move(rp), std::move(ci)));
         CK(upload(c->gen_K, v.data(), nnz, c->stream));
         CK(c->gen_LU.reserve(nnz));
         CK(c->gen_diag.reserve(n));

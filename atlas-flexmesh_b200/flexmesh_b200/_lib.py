@@ -33,7 +33,7 @@ EXPORTS = [
     "fm_profile_enable", "fm_profile_read", "fm_newton_config_default", "fm_newton_step_cfg",
     "fm_newton_history", "fm_set_wait_limit", "fm_check_wait", "fm_newton_step_cfg_host",
     "fm_newton_solve_cfg", "fm_element_states", "fm_set_state_output", "fm_checkpoint_save",
-    "fm_checkpoint_header", "fm_checkpoint_load",
+    "fm_checkpoint_header", "fm_checkpoint_load", "fm_mesh_coloring",
 ]
 PROF_KINDS = {0: "assemble", 1: "ilu0", 2: "trsv", 3: "spmv", 4: "vector", 5: "states"}
 
@@ -80,6 +80,17 @@ _CK_ARRAYS = [("xyz", np.float64, "n", 3), ("node_disp", np.float64, "n", 3),
               ("F", np.float64, "e", 9), ("stress", np.float64, "e", 6),
               ("eps_plastic", np.float64, "e", 6), ("kappa", np.float64, "e", 1),
               ("gamma_p", np.float64, "e", 1), ("u", np.float64, "d", 1)]
+
+
+def mesh_coloring(n_nodes, conn):
+    """fm_mesh_coloring: (colors per tet, colour count) of MeshColoring::compute"""
+    conn = np.ascontiguousarray(conn, np.uint32)
+    colors = np.zeros(conn.size // 4, np.uint32)
+    nc = _u32()
+    st = lib().fm_mesh_coloring(n_nodes, conn.size // 4, _hp(conn), _hp(colors), C.byref(nc))
+    if st:
+        raise FMError(st, "fm_mesh_coloring")
+    return colors, nc.value
 
 
 def save_checkpoint(path, xyz, conn, u, load_step=0, adapt_iter=0, **arrays):
@@ -184,6 +195,7 @@ def lib() -> C.CDLL:
             "fm_checkpoint_save": [C.c_char_p, _P(Checkpoint)],
             "fm_checkpoint_header": [C.c_char_p, _P(Checkpoint)],
             "fm_checkpoint_load": [C.c_char_p, _P(Checkpoint)],
+            "fm_mesh_coloring": [_u32, _u32, _vp, _vp, _P(_u32)],
             "fm_set_wait_limit": [_vp, _u64],
             "fm_check_wait": [_vp],
             "fm_profile_enable": [_vp, _i32],

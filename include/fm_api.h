@@ -133,11 +133,21 @@ fm_status fm_unit_cube(int N, double* xyz, uint32_t* conn);
  * (FEM/fem_types.hpp:168-211).  elem_volume, if given, is the stored
  * TetraElement::volume: elements with volume < 1e-30 are skipped exactly as
  * assemble_global_threadlocal skips them (FEM/adaptive_fem_engine.hpp:1169);
- * NULL uses |det J|/6 of the given coordinates.  Builds the node neighbour
- * structure, the solve-pattern CSR and the ILU(0) dependency schedules on
- * the host and uploads them. */
+ * NULL uses |det J|/6 of the given coordinates.  Builds the node->tet
+ * incidence, the node neighbour sets, the ILU(0) dependency levels and
+ * schedules and the assembly's scatter structure on the device (the
+ * reference builds its neighbour sets per node with std::set, :1076-1085),
+ * and the triangular-solve plan on the host.  Clears the flags. */
 fm_status fm_set_mesh(fm_ctx* ctx, uint32_t n_nodes, const double* xyz, uint32_t n_elems,
                       const uint32_t* conn, const double* elem_volume);
+
+/* Replaces MeshColoring::compute (FEM/adaptive_fem_engine.hpp:1549-1602)
+ * (host only): greedy first-fit element colouring in element order, tets
+ * sharing a node get different colours; the same colours as the
+ * reference's all-pairs construction in time linear in the incidences.
+ * colors[n_elems]; *n_colors = 1 + the largest colour (0 for no tets). */
+fm_status fm_mesh_coloring(uint32_t n_nodes, uint32_t n_elems, const uint32_t* conn,
+                           uint32_t* colors, uint32_t* n_colors);
 
 /* Replaces build_csr_sparsity_pattern_rigorous (FEM/adaptive_fem_engine.hpp:1069)
  * and the element->CSR lookup it feeds (:1141-1150).  Any output may be NULL.

@@ -135,6 +135,9 @@ def ref():
         R.ref_pcg_ilu0.argtypes = [u32, _u32p, _u32p, _f64p, _f64p, _f64p, f64, i32, i32]
         R.ref_pcg_ilu0.restype = i32
         R.ref_spmv.argtypes = [u32, _u32p, _u32p, _f64p, _f64p, _f64p]
+        if hasattr(R, "ref_mesh_coloring"):
+            R.ref_mesh_coloring.argtypes = [u32, _f64p, u32, _u32p, _f64p, _u32p]
+            R.ref_mesh_coloring.restype = u32
         if hasattr(R, "ref_checkpoint_save"):
             R.ref_checkpoint_save.argtypes = [C.c_char_p, i32, _f64p, _opt(_f64p), _opt(_f64p),
                                               u32, u32]

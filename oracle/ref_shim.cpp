@@ -220,6 +220,15 @@ void ref_spmv(uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx, cons
     A.matvec(x, y);
 }
 
+// MeshColoring::compute (:1554), O(E^2): small meshes only
+uint32_t ref_mesh_coloring(uint32_t n_nodes, const double* xyz, uint32_t n_elems,
+                           const uint32_t* conn, const double* vol, uint32_t* colors) {
+    MeshTopology m = mesh_from_arrays(n_nodes, xyz, n_elems, conn, vol);
+    const MeshColoring mc = MeshColoring::compute(m);
+    std::memcpy(colors, mc.element_colors.data(), sizeof(uint32_t) * n_elems);
+    return mc.n_colors;
+}
+
 // sl3_retraction(G, 0) (CORE/lie_operator.cpp:300) on a Matrix3x3 whose
 // data array is G9
 void ref_sl3_retraction(const double* G9, double* out9) {

@@ -184,3 +184,23 @@ def test_flattened_element_takes_the_reference_guarded_inverse(fm):
     assert np.abs(fo).max() > 1e20  # the guarded branch was taken
     assert np.abs(f - fo).max() <= 1e-12 * np.abs(fo).max()
     assert np.abs(K - Ko).max() <= 1e-12 * np.abs(Ko).max()
+
+
+def test_valence_beyond_the_kernels_limit_is_refused(fm):
+    """a node shared by 40 tets (the kernels hold at most 32 incident tets
+    and 32 neighbours per node): fm_set_mesh refuses with FM_ERR_LIMITS"""
+    k = 40
+    ang = np.linspace(0, 2 * np.pi, k, endpoint=False)
+    ring = np.stack([np.cos(ang), np.sin(ang), np.zeros(k)], 1)
+    xyz = np.concatenate([[[0, 0, 0], [0, 0, 1]], ring]).reshape(-1)
+    conn = np.array([[0, 1, 2 + i, 2 + (i + 1) % k] for i in range(k)], np.uint32).reshape(-1)
+    ctx = fm.Context(0)
+    with pytest.raises(fm.FMError) as e:
+        ctx.set_mesh(xyz, conn)
+    assert e.value.status == 9 and "valence" in str(e.value)
+    # the context takes a valid mesh afterwards
+    from flexmesh_b200 import configs
+
+    P = configs.small_block(2)
+    ctx.set_mesh(P.xyz, P.conn)
+    assert ctx.n_nodes == P.n_nodes
