@@ -33,13 +33,18 @@ def cu(a):
     return torch.as_tensor(np.ascontiguousarray(a), device="cuda")
 
 
-@pytest.mark.parametrize("N", [6, 12])
-def test_noalloc_apply_matches_ilu0_apply(fm, N):
+@pytest.mark.parametrize("N,path", [(6, "push"), (12, "push"), (6, "pipe")])
+def test_noalloc_apply_matches_ilu0_apply(fm, monkeypatch, N, path):
+    """path: the triangular solves the context plans at fm_set_mesh (the
+    slab-partitioned push solves, or the grid-wide pipelined ones that
+    meshes beyond the push plan's limits use); the static scratch serves both"""
     from flexmesh_b200 import configs
 
     P = configs.small_block(N)
+    monkeypatch.setenv("FM_TRSV_PATH", path)
     ctx = fm.Context(0)
     ctx.set_mesh(P.xyz, P.conn)
+    monkeypatch.delenv("FM_TRSV_PATH", raising=False)
     ctx.set_material(1.0, P.nu)
     ctx.set_bc(P.mask, P.bc_value)
     u = 0.01 * np.random.default_rng(3).standard_normal(P.xyz.size)
