@@ -103,6 +103,11 @@ struct fm_ctx {
     DevBuf<double> ke_scratch;
     DevBuf<unsigned char> elem_rec;  // assembly element-pass records
     DevBuf<uint32_t> inc_pos, nbr_members;  // node-pass scatter structure
+    // pipelined assembly plan (tasks, node order, per-chunk task counts, counters)
+    DevBuf<uint4> pipe_tasks;
+    DevBuf<uint32_t> pipe_order, pipe_entasks, pipe_nntasks;
+    DevBuf<unsigned> pipe_counters;
+    fm::AsmPipe pipe[2];
 
     // solver state
     Work<double> w64;
@@ -288,6 +293,8 @@ fm::MeshDev mesh_view(const fm_ctx* c) {
     m.elem_rec = c->elem_rec.p;
     m.inc_pos = c->inc_pos.p;
     m.nbr_members = c->nbr_members.p;
+    m.pipe[0] = c->pipe[0];
+    m.pipe[1] = c->pipe[1];
     return m;
 }
 
@@ -630,6 +637,41 @@ fm_status ensure_dof_levels(fm_ctx* c) {
     return FM_OK;
 }
 
+// Plan of the pipelined assembly (fm_kernels.hpp AsmPipe): element chunks
+// of 2^14 tets, whose records (3.7 MB FP64) and ring stay in L2.  The
+// default; FM_ASM_PATH=split keeps the element and node passes as two
+// launches.
+fm_status setup_assemble_pipe(fm_ctx* c) {
+    c->pipe[0] = c->pipe[1] = fm::AsmPipe();
+    const char* path = getenv("FM_ASM_PATH");
+    if (path && std::strcmp(path, "split") == 0) return FM_OK;
+    constexpr uint32_t kShift = 14;
+    fm::AsmPipePlan plan;
+    CK(fm::plan_assemble_pipe(c->nn, c->ne, c->inc_ptr.p, c->inc_e.p, kShift, plan, c->stream));
+    if (plan.tasks.empty()) return FM_OK;
+    CK(upload(c->pipe_tasks, plan.tasks.data(), plan.tasks.size(), c->stream));
+    CK(upload(c->pipe_order, plan.node_order.data(), plan.node_order.size(), c->stream));
+    CK(upload(c->pipe_entasks, plan.elem_ntasks.data(), plan.elem_ntasks.size(), c->stream));
+    CK(upload(c->pipe_nntasks, plan.node_ntasks.data(), plan.node_ntasks.size(), c->stream));
+    CK(c->pipe_counters.reserve(1 + 2 * (size_t)plan.n_chunks));
+    for (int k = 0; k < 2; ++k) {
+        fm::AsmPipe& P = c->pipe[k];
+        P.tasks = c->pipe_tasks.p;
+        P.n_tasks = (uint32_t)plan.tasks.size();
+        P.node_order = c->pipe_order.p;
+        P.elem_ntasks = c->pipe_entasks.p;
+        P.node_ntasks = c->pipe_nntasks.p;
+        P.n_chunks = plan.n_chunks;
+        P.shift = kShift;
+        P.slots = plan.slots;
+        P.span = plan.span;
+        P.counters = c->pipe_counters.p;
+        P.grid = fm::assemble_pipe_grid(c->device, k == 1);
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return FM_OK;
+}
+
 // element -> CSR slot maps on the device (chunks of 2^20 tets through a
 // scratch buffer): into host memory, or into a device buffer
 fm_status slot_map_device(fm_ctx* c, int reference, int32_t* host_out, DevBuf<int32_t>* dev_out) {
@@ -855,6 +897,7 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
         for (size_t l = 0; l + 1 < c->node_up.size(); ++l)
             c->width_bwd = std::max(c->width_bwd, c->node_up[l + 1] - c->node_up[l]);
         TRY(setup_push_solves(c, c->node_lp, c->node_lo, c->node_up, c->node_uo));
+        TRY(setup_assemble_pipe(c));
         CK(cudaStreamSynchronize(c->stream));
         CK(c->done.reserve(std::max<size_t>(c->done.n, (size_t)c->nn + 1)));
         CK(cudaMemsetAsync(c->done.p, 0, c->done.n * sizeof(unsigned), c->stream));
@@ -1323,7 +1366,7 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
         if (!c->state_F || !c->state_stress) return;
         PROF(FM_PROF_STATES, 1);
         fm::launch_element_states(m, u, c->nu, c->state_F, c->state_stress,
-                                  &c->sc.p->state_violations, c->status(), c->stream);
+                                  c->sc.p->state_counts, c->stream);
     };
 
     auto finish = [&](fm_status st) -> fm_status {
@@ -1473,19 +1516,20 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
 }
 
 fm_status fm_element_states(fm_ctx* c, const double* u, double* F, double* stress,
-                            uint32_t* det_violations) {
+                            uint32_t* det_violations, uint32_t* nonfinite) {
     TRY(need_material(c));
     if (!u || !F || !stress) return fail(c, FM_ERR_ARG, "null argument");
-    CK(cudaMemsetAsync(&c->sc.p->state_violations, 0, sizeof(unsigned), c->stream));
+    CK(cudaMemsetAsync(c->sc.p->state_counts, 0, 2 * sizeof(unsigned), c->stream));
     {
         PROF(FM_PROF_STATES, 1);
-        fm::launch_element_states(mesh_view(c), u, c->nu, F, stress, &c->sc.p->state_violations,
-                                  c->status(), c->stream);
+        fm::launch_element_states(mesh_view(c), u, c->nu, F, stress, c->sc.p->state_counts,
+                                  c->stream);
     }
     CK(cudaGetLastError());
     TRY(sync_scalars(c));
-    if (det_violations) *det_violations = c->h_sc->state_violations;
-    return check_flags(c, c->h_sc->status, "fm_element_states");
+    if (det_violations) *det_violations = c->h_sc->state_counts[0];
+    if (nonfinite) *nonfinite = c->h_sc->state_counts[1];
+    return FM_OK;
 }
 
 fm_status fm_set_state_output(fm_ctx* c, double* F, double* stress) {

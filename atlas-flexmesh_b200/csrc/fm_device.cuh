@@ -39,7 +39,7 @@ struct DevScalars {
     unsigned wait_budget;  // bounded-wait limit in 1024 cycles (0: kWaitCycles); follows status
     unsigned counter[8];  // last-block counters (one per reduction site)
     unsigned never;       // a flag no kernel sets (fm_check_wait waits on it)
-    unsigned state_violations;  // element state update: |det F_sl3 - 1| > 1e-8 count
+    unsigned state_counts[2];   // element state update: |det F_sl3 - 1| > 1e-8, non-finite
 };
 
 constexpr int kRedBlocks = 296;  // 2 x 148 SMs: fixed grid => fixed summation order
@@ -246,6 +246,27 @@ struct Mandel {
     double lnJ;
 };
 
+// |det C| < 1e-30 for C = F^T F, each operation rounded as the reference's
+// neo_hookean_response and matrix_3x3_inv round it (:88-96, :53-56)
+static __device__ __noinline__ bool degenerate_c(double f0, double f1, double f2, double f3,
+                                                  double f4, double f5, double f6, double f7,
+                                                  double f8) {
+    const double F[9] = {f0, f1, f2, f3, f4, f5, f6, f7, f8};
+    double C[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double acc = 0.0;
+            for (int k = 0; k < 3; ++k) acc = __dadd_rn(acc, __dmul_rn(F[k * 3 + i], F[k * 3 + j]));
+            C[i * 3 + j] = acc;
+        }
+    const double t0 = __dsub_rn(__dmul_rn(C[4], C[8]), __dmul_rn(C[7], C[5]));
+    const double t1 = __dsub_rn(__dmul_rn(C[1], C[8]), __dmul_rn(C[7], C[2]));
+    const double t2 = __dsub_rn(__dmul_rn(C[1], C[5]), __dmul_rn(C[4], C[2]));
+    const double det =
+        __dadd_rn(__dsub_rn(__dmul_rn(C[0], t0), __dmul_rn(C[3], t1)), __dmul_rn(C[6], t2));
+    return fabs(det) < 1e-30;
+}
+
 __device__ __forceinline__ Mandel mandel_stress(const double F[9], double J, double mu, double lam) {
     Mandel M;
     const double c00 = F[0] * F[0] + F[3] * F[3] + F[6] * F[6];
@@ -257,10 +278,13 @@ __device__ __forceinline__ Mandel mandel_stress(const double F[9], double J, dou
     const double Js = J < kJSafe ? kJSafe : J;
     M.lnJ = log(Js);
     const double vol = lam * M.lnJ;
-    if (J * J < 1e-30) {
-        // det C = J^2 below matrix_3x3_inv's 1e-30 guard (:56-60): the
-        // reference's C^-1 is then 1e30 I, S = (mu (1 - 1e30) + lam lnJ 1e30) I
-        // and M = C S
+    // det C = J^2 below matrix_3x3_inv's 1e-30 guard (:56-60) makes the
+    // reference's C^-1 1e30 I, S = (mu (1 - 1e30) + lam lnJ 1e30) I and
+    // M = C S.  Near a singular F the guard sees det C through its own
+    // rounding, so there the decision is taken on det C formed as the
+    // reference forms it (C_ij = sum_k F_ki F_kj, cofactor expansion,
+    // no fused operations)
+    if (J * J < 1e-10 && degenerate_c(F[0], F[1], F[2], F[3], F[4], F[5], F[6], F[7], F[8])) {
         const double s = mu * (1.0 - 1e30) + vol * 1e30;
         M.m00 = s * c00;
         M.m11 = s * c11;

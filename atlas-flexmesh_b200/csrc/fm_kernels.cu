@@ -13,6 +13,7 @@
 // triangular solves: a persistent grid walks the rows in a topological
 // order (dependency levels); each row waits on its dependencies' release
 // flags with a bounded spin, so there is no per-level launch or barrier.
+#include <algorithm>
 #include <cstdio>
 
 #include "fm_kernels.hpp"
@@ -77,6 +78,93 @@ struct __align__(16) ElemRec<float> {
 static_assert(sizeof(ElemRec<double>) <= kElemRecBytes && sizeof(ElemRec<double>) % 16 == 0, "");
 static_assert(sizeof(ElemRec<float>) <= kElemRecBytes && sizeof(ElemRec<float>) % 16 == 0, "");
 
+// 16-byte stores of a whole record from registers
+__device__ __forceinline__ void store_rec(ElemRec<double>* dst, const ElemRec<double>& r) {
+    double2* f = reinterpret_cast<double2*>(dst->f);
+    double2* d = reinterpret_cast<double2*>(dst->d);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        f[i] = make_double2(r.f[2 * i], r.f[2 * i + 1]);
+        d[i] = make_double2(r.d[2 * i], r.d[2 * i + 1]);
+    }
+    double2* t = reinterpret_cast<double2*>(dst->s);
+    t[0] = make_double2(r.s[0], r.s[1]);
+    t[1] = make_double2(r.s[2], r.active);
+}
+__device__ __forceinline__ void store_rec(ElemRec<float>* dst, const ElemRec<float>& r) {
+    double2* f = reinterpret_cast<double2*>(dst->f);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) f[i] = make_double2(r.f[2 * i], r.f[2 * i + 1]);
+    float4* d = reinterpret_cast<float4*>(dst->d);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) d[i] = make_float4(r.d[4 * i], r.d[4 * i + 1], r.d[4 * i + 2], r.d[4 * i + 3]);
+    *reinterpret_cast<float4*>(dst->s) = make_float4(r.s[0], r.s[1], r.s[2], r.active);
+}
+
+// One tet of the element pass: kinematics, Mandel stress, the four vertex
+// forces (FP64) and, with_k, the tangent scalars and shape gradients in the
+// tangent's type, stored as one 16-byte-aligned record.  Returns the flags.
+template <typename KT>
+__device__ __forceinline__ unsigned asm_element(const MeshDev& m, const double* __restrict__ u,
+                                                uint32_t e, ElemRec<KT>* dst_rec, int with_k) {
+    unsigned flags = 0;
+    uint4 c = m.conn[e];
+    const bool active = !(c.x & 0x80000000u);
+    c.x &= 0x7fffffffu;
+    const uint32_t cn[4] = {c.x, c.y, c.z, c.w};
+    ElemRec<KT> r;
+#pragma unroll
+    for (int i = 0; i < 12; ++i) {
+        r.f[i] = 0.0;
+        r.d[i] = KT(0);
+    }
+    r.s[0] = r.s[1] = r.s[2] = KT(0);
+    r.active = KT(0);
+    if (active) {
+        double x[12], ue[12];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                x[3 * a + d] = __ldg(m.xyz + 3 * (size_t)cn[a] + d);
+                ue[3 * a + d] = __ldg(u + 3 * (size_t)cn[a] + d);
+            }
+        TetKin k;
+        if (tet_kinematics(x, ue, k)) {
+            double mu, lam;
+            material_of(m.mat_mode, m.m0, m.m1, e, m.mu_s, m.lam_s, m.c_mu, m.c_lam, mu, lam);
+            const Mandel M = mandel_stress(k.F, k.J, mu, lam);
+            double fs = 0.0;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const double* dI = k.d[a];
+                r.f[3 * a + 0] = k.vol * (M.m00 * dI[0] + M.m01 * dI[1] + M.m02 * dI[2]);
+                r.f[3 * a + 1] = k.vol * (M.m01 * dI[0] + M.m11 * dI[1] + M.m12 * dI[2]);
+                r.f[3 * a + 2] = k.vol * (M.m02 * dI[0] + M.m12 * dI[1] + M.m22 * dI[2]);
+                fs += r.f[3 * a] + r.f[3 * a + 1] + r.f[3 * a + 2];
+            }
+            if (!(k.J > 0.0)) flags |= FM_FLAG_INVERTED;
+            if (k.J < kJSafe) flags |= FM_FLAG_J_CLAMPED;
+            if (!isfinite(fs)) flags |= FM_FLAG_NONFINITE;
+            if (with_k) {
+                double a, b;
+                tangent_ab(mu, lam, k.J, M.lnJ, m.inv_cnu, a, b);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) r.d[3 * q + d] = (KT)k.d[q][d];
+                r.s[0] = (KT)(k.vol * a);
+                r.s[1] = (KT)(k.vol * b);
+                r.s[2] = (KT)(k.vol * mu);
+                if (!isfinite(a + b)) flags |= FM_FLAG_NONFINITE;
+            }
+            r.active = KT(1);
+        }
+    }
+    store_rec(dst_rec, r);
+    return flags;
+}
+
 // Element pass: one thread per tet.  with_k = 0 (residual only) skips the
 // tangent scalars and gradients.
 template <typename KT>
@@ -85,84 +173,38 @@ __global__ void __launch_bounds__(128, 4)
                    int with_k, unsigned* __restrict__ status) {
     unsigned flags = 0;
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < m.n_elems;
-         e += gridDim.x * blockDim.x) {
-        uint4 c = m.conn[e];
-        const bool active = !(c.x & 0x80000000u);
-        c.x &= 0x7fffffffu;
-        const uint32_t cn[4] = {c.x, c.y, c.z, c.w};
-        ElemRec<KT> r;
-#pragma unroll
-        for (int i = 0; i < 12; ++i) {
-            r.f[i] = 0.0;
-            r.d[i] = KT(0);
-        }
-        r.s[0] = r.s[1] = r.s[2] = KT(0);
-        r.active = KT(0);
-        if (active) {
-            double x[12], ue[12];
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    x[3 * a + d] = __ldg(m.xyz + 3 * (size_t)cn[a] + d);
-                    ue[3 * a + d] = __ldg(u + 3 * (size_t)cn[a] + d);
-                }
-            TetKin k;
-            if (tet_kinematics(x, ue, k)) {
-                double mu, lam;
-                material_of(m.mat_mode, m.m0, m.m1, e, m.mu_s, m.lam_s, m.c_mu, m.c_lam, mu, lam);
-                const Mandel M = mandel_stress(k.F, k.J, mu, lam);
-                double fs = 0.0;
-#pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                    const double* dI = k.d[a];
-                    r.f[3 * a + 0] = k.vol * (M.m00 * dI[0] + M.m01 * dI[1] + M.m02 * dI[2]);
-                    r.f[3 * a + 1] = k.vol * (M.m01 * dI[0] + M.m11 * dI[1] + M.m12 * dI[2]);
-                    r.f[3 * a + 2] = k.vol * (M.m02 * dI[0] + M.m12 * dI[1] + M.m22 * dI[2]);
-                    fs += r.f[3 * a] + r.f[3 * a + 1] + r.f[3 * a + 2];
-                }
-                if (!(k.J > 0.0)) flags |= FM_FLAG_INVERTED;
-                if (k.J < kJSafe) flags |= FM_FLAG_J_CLAMPED;
-                if (!isfinite(fs)) flags |= FM_FLAG_NONFINITE;
-                if (with_k) {
-                    double a, b;
-                    tangent_ab(mu, lam, k.J, M.lnJ, m.inv_cnu, a, b);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q)
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) r.d[3 * q + d] = (KT)k.d[q][d];
-                    r.s[0] = (KT)(k.vol * a);
-                    r.s[1] = (KT)(k.vol * b);
-                    r.s[2] = (KT)(k.vol * mu);
-                    if (!isfinite(a + b)) flags |= FM_FLAG_NONFINITE;
-                }
-                r.active = KT(1);
-            }
-        }
-        // 16-byte stores of the whole record
-        const float4* src = reinterpret_cast<const float4*>(&r);
-        float4* dst = reinterpret_cast<float4*>(rec + e);
-#pragma unroll
-        for (int i = 0; i < (int)(sizeof(ElemRec<KT>) / 16); ++i) dst[i] = src[i];
-    }
+         e += gridDim.x * blockDim.x)
+        flags |= asm_element<KT>(m, u, e, rec + e, with_k);
     if (flags) raise_flag(status, flags);
 }
 
-// Node pass: one warp owns one node.  Lane l < mi stages incident tet l's
-// record (gradients, the owner's vertex force, tangent scalars) in shared
-// memory; lane k then forms block (n, nbr[k]).
-template <typename KT>
-__global__ void __launch_bounds__(kAsmWarps * 32, 3)
-    k_assemble(MeshDev m, const ElemRec<KT>* __restrict__ rec, KT* __restrict__ K,
-               double* __restrict__ f, double* __restrict__ R, int apply_bc,
-               unsigned* __restrict__ status) {
-    (void)status;
-    __shared__ AsmStage<KT> stage[kAsmWarps];
-    const int lane = threadIdx.x & 31;
-    const int wi = threadIdx.x >> 5;
-    const uint32_t n = blockIdx.x * kAsmWarps + wi;
-    if (n >= m.n_nodes) return;  // uniform per warp
-    AsmStage<KT>& S = stage[wi];
+// Where element e's record lives: rec + e, or, for the pipelined assembly,
+// in a ring of `slots` chunks of 2^shift records (chunk c in slot c % slots).
+struct RecRing {
+    uint32_t shift = 31, slots = 0;  // slots == 0: no ring
+    __device__ __forceinline__ size_t index(uint32_t e) const {
+        if (!slots) return e;
+        const uint32_t c = e >> shift;
+        return ((size_t)(c % slots) << shift) | (e & ((1u << shift) - 1u));
+    }
+};
+
+// a record field: a plain load, or an L2 load (records written during the
+// same kernel by other SMs must not come from a stale L1 line)
+template <bool kL2, typename T>
+__device__ __forceinline__ T rec_ld(const T* p) {
+    if constexpr (kL2) return __ldcg(p);
+    else return *p;
+}
+
+// Node pass for one node: one warp owns it.  Lane l < mi stages incident
+// tet l's record (gradients, the owner's vertex force, tangent scalars) in
+// shared memory; lane k then forms block (n, nbr[k]).
+template <typename KT, bool kL2>
+__device__ __forceinline__ void asm_node(const MeshDev& m, const ElemRec<KT>* __restrict__ rec,
+                                         RecRing ring, uint32_t n, KT* __restrict__ K,
+                                         double* __restrict__ f, double* __restrict__ R,
+                                         int apply_bc, AsmStage<KT>& S, int lane) {
 
     const uint32_t nb0 = m.nbr_ptr[n];
     const int deg = (int)(m.nbr_ptr[n + 1] - nb0);
@@ -178,25 +220,25 @@ __global__ void __launch_bounds__(kAsmWarps * 32, 3)
     if (lane < mi) {
         const uint32_t e = __ldg(m.inc + e0 + lane);
         packed = __ldg(m.inc_pos + e0 + lane);
-        const ElemRec<KT>& r = rec[e];
-        const bool act = r.active != KT(0);
+        const ElemRec<KT>& r = rec[ring.index(e)];
+        const bool act = rec_ld<kL2>(&r.active) != KT(0);
         if (act) {
             const int il = byte_index(packed, (uint32_t)self_k);
-            fi0 = r.f[3 * il];
-            fi1 = r.f[3 * il + 1];
-            fi2 = r.f[3 * il + 2];
+            fi0 = rec_ld<kL2>(&r.f[3 * il]);
+            fi1 = rec_ld<kL2>(&r.f[3 * il + 1]);
+            fi2 = rec_ld<kL2>(&r.f[3 * il + 2]);
         }
         if (K != nullptr) {
             // an inactive tet (degenerate at this state) stays in the edge
             // lists with zero data: it adds exact zeros
 #pragma unroll
-            for (int q = 0; q < 12; ++q) S.d[lane][q] = act ? r.d[q] : KT(0);
+            for (int q = 0; q < 12; ++q) S.d[lane][q] = act ? rec_ld<kL2>(&r.d[q]) : KT(0);
             S.fI[lane][0] = (KT)fi0;
             S.fI[lane][1] = (KT)fi1;
             S.fI[lane][2] = (KT)fi2;
-            S.vabm[lane][0] = act ? r.s[0] : KT(0);
-            S.vabm[lane][1] = act ? r.s[1] : KT(0);
-            S.vabm[lane][2] = act ? r.s[2] : KT(0);
+            S.vabm[lane][0] = act ? rec_ld<kL2>(&r.s[0]) : KT(0);
+            S.vabm[lane][1] = act ? rec_ld<kL2>(&r.s[1]) : KT(0);
+            S.vabm[lane][2] = act ? rec_ld<kL2>(&r.s[2]) : KT(0);
         }
     }
     S.pos[lane] = packed;
@@ -270,10 +312,120 @@ __global__ void __launch_bounds__(kAsmWarps * 32, 3)
 }
 
 template <typename KT>
+__global__ void __launch_bounds__(kAsmWarps * 32, 3)
+    k_assemble(MeshDev m, const ElemRec<KT>* __restrict__ rec, KT* __restrict__ K,
+               double* __restrict__ f, double* __restrict__ R, int apply_bc,
+               unsigned* __restrict__ status) {
+    (void)status;
+    __shared__ AsmStage<KT> stage[kAsmWarps];
+    const int lane = threadIdx.x & 31;
+    const int wi = threadIdx.x >> 5;
+    const uint32_t n = blockIdx.x * kAsmWarps + wi;
+    if (n >= m.n_nodes) return;  // uniform per warp
+    asm_node<KT, false>(m, rec, RecRing{}, n, K, f, R, apply_bc, stage[wi], lane);
+}
+
+// Bounded wait until *cnt reaches target (acquire); FM_FLAG_TIMEOUT on expiry.
+__device__ __forceinline__ void wait_count(const unsigned* cnt, unsigned target,
+                                           unsigned* status) {
+    if (ld_acquire(cnt) >= target) return;
+    const long long t0 = clock64(), limit = wait_limit(status);
+    for (unsigned it = 1;; ++it) {
+        if (ld_acquire(cnt) >= target) return;
+        if ((it & 31u) == 0) {
+            if (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) return;
+            if (clock64() - t0 > limit) {
+                raise_flag(status, FM_FLAG_TIMEOUT);
+                return;
+            }
+        }
+    }
+}
+
+constexpr int kPipeThreads = kAsmWarps * 32;
+
+// The pipelined assembly: see AsmPipe.  Thread 0 draws a ticket and waits
+// for the task's inputs; the block runs the task; every thread fences its
+// writes before thread 0 counts the task done.
+template <typename KT>
+__global__ void __launch_bounds__(kPipeThreads, 2)
+    k_assemble_pipe(MeshDev m, AsmPipe P, const double* __restrict__ u,
+                    ElemRec<KT>* __restrict__ rec, KT* __restrict__ K, double* __restrict__ f,
+                    double* __restrict__ R, int apply_bc, unsigned* __restrict__ status) {
+    __shared__ AsmStage<KT> stage[kAsmWarps];
+    __shared__ uint4 task_s;
+    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+    const RecRing ring{P.shift, P.slots};
+    unsigned* const ticket = P.counters;
+    unsigned* const edone = P.counters + 1;
+    unsigned* const ndone = P.counters + 1 + P.n_chunks;
+    unsigned flags = 0;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(ticket, 1u);
+            uint4 tk = t < P.n_tasks ? P.tasks[t] : make_uint4(~0u, 0u, 0u, 0u);
+            if (tk.x != ~0u) {
+                const uint32_t c = tk.x & 0x7fffffffu;
+                if (tk.x >> 31) {
+                    for (uint32_t cc = c > P.span ? c - P.span : 0; cc <= c; ++cc)
+                        wait_count(edone + cc, P.elem_ntasks[cc], status);
+                } else if (P.slots && c >= P.slots) {
+                    for (uint32_t cc = c - P.slots; cc + 2 <= c; ++cc)
+                        wait_count(ndone + cc, P.node_ntasks[cc], status);
+                }
+                __threadfence();
+            }
+            task_s = tk;
+        }
+        __syncthreads();
+        const uint4 tk = task_s;
+        __syncthreads();  // task_s is rewritten only after every thread read it
+        if (tk.x == ~0u) break;
+        const bool node = (tk.x >> 31) != 0;
+        if (!node) {
+            for (uint32_t e = tk.y + threadIdx.x; e < tk.z; e += blockDim.x)
+                flags |= asm_element<KT>(m, u, e, rec + ring.index(e), K != nullptr);
+        } else {
+            for (uint32_t q = tk.y + (uint32_t)wi; q < tk.z; q += kAsmWarps)
+                asm_node<KT, true>(m, rec, ring, __ldg(P.node_order + q), K, f, R, apply_bc,
+                                   stage[wi], lane);
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) atomicAdd((node ? ndone : edone) + (tk.x & 0x7fffffffu), 1u);
+    }
+    if (flags) raise_flag(status, flags);
+}
+
+int assemble_pipe_grid(int device, bool fp32) {
+    int per_sm = 0, sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const cudaError_t e =
+        fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_assemble_pipe<float>,
+                                                             kPipeThreads, 0)
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_assemble_pipe<double>,
+                                                             kPipeThreads, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return per_sm * sms;
+}
+
+template <typename KT>
 static void launch_assemble_t(const MeshDev& m, const double* u, KT* K, double* f, double* R,
                               int apply_bc, unsigned* status, cudaStream_t s) {
     if (m.n_nodes == 0) return;
     ElemRec<KT>* rec = static_cast<ElemRec<KT>*>(m.elem_rec);
+    const AsmPipe* pipe = &m.pipe[sizeof(KT) == 4 ? 1 : 0];
+    if (pipe->n_tasks && pipe->grid > 0) {
+        cudaMemsetAsync(pipe->counters, 0, sizeof(unsigned) * (1 + 2 * (size_t)pipe->n_chunks),
+                        s);
+        const unsigned grid = std::min<unsigned>((unsigned)pipe->grid, pipe->n_tasks);
+        k_assemble_pipe<KT><<<grid, kPipeThreads, 0, s>>>(m, *pipe, u, rec, K, f, R, apply_bc,
+                                                          status);
+        return;
+    }
     if (m.n_elems) {
         unsigned ge = (m.n_elems + 127) / 128;
         if (ge > 148u * 32u) ge = 148u * 32u;

@@ -8,6 +8,26 @@
 
 namespace fm {
 
+// Plan of the pipelined assembly (one launch): the element pass and the node
+// pass run as interleaved tasks handed out by ticket, E(0), N(0), E(1), ...
+// E(c) evaluates element chunk c (2^shift tets) into a record ring of
+// `slots` chunks (0: no ring, records at their element index); N(c) runs the
+// node pass of the nodes whose last incident tet lies in chunk c.  A node
+// task waits for element chunks c - span .. c (span: the most chunks a
+// node's incident tets spread over, minus one); an element task whose ring
+// slot is in use waits for the node chunks that read it.  Every wait is on
+// a task with an earlier ticket, bounded by the status word's limit.
+struct AsmPipe {
+    const uint4* tasks = nullptr;          // {node << 31 | chunk, begin, end, 0}
+    uint32_t n_tasks = 0;
+    const uint32_t* node_order = nullptr;  // node positions of the node tasks
+    const uint32_t* elem_ntasks = nullptr; // tasks per chunk
+    const uint32_t* node_ntasks = nullptr;
+    uint32_t n_chunks = 0, shift = 14, slots = 0, span = 0;
+    unsigned* counters = nullptr;          // [0] ticket, [1 + c] element, [1 + Q + c] node
+    int grid = 0;
+};
+
 // Mesh/material data resident on the device (read by assembly kernels).
 struct MeshDev {
     uint32_t n_nodes = 0, n_elems = 0;
@@ -33,18 +53,25 @@ struct MeshDev {
     // l-th incident tet (not skipped) holds the edge to neighbour entry j
     const uint32_t* inc_pos = nullptr;
     const uint32_t* nbr_members = nullptr;
+    // pipelined assembly plans, FP64 [0] and FP32 tangent [1] (n_tasks == 0:
+    // the two-launch form)
+    AsmPipe pipe[2];
 };
 constexpr size_t kElemRecBytes = 224;
+
 
 // A10/A11/A12: assembly in two passes, an element pass (each tet's
 // kinematics, stress, vertex forces and tangent scalars, once) and a
 // node-owner pass that writes every CSR row block once.  K (double or float,
 // may be null for a residual-only call), f (FP64, may be null), R = -f with
 // zeros on constrained DOFs (may be null).  m.elem_rec is required.
+// The pipelined single launch where m.pipe has a plan, else two launches.
 void launch_assemble(const MeshDev& m, const double* u, double* K, double* f, double* R,
                      int apply_bc, unsigned* status, cudaStream_t s);
 void launch_assemble(const MeshDev& m, const double* u, float* K, double* f, double* R,
                      int apply_bc, unsigned* status, cudaStream_t s);
+// resident blocks of the pipelined assembly kernel on this device
+int assemble_pipe_grid(int device, bool fp32);
 // Element-centric scatter through an int32 slot map (reference pattern).
 // K and f must be zeroed by the caller; Ke_scratch holds 144*n_elems doubles.
 void launch_assemble_slotmap(const MeshDev& m, const double* u, const int32_t* slot, double* K,
@@ -145,10 +172,10 @@ void launch_f32_to_f64_scaled(uint32_t n, const float* x, double scale, double* 
 // Element state update (fm_states.cu): per element F_sl3 (9, the
 // reference's column-major Matrix3x3 data) and Mandel stress (6); elements
 // with a degenerate reference Jacobian keep their previous state.
-// violations (nullable) counts |det F_sl3 - 1| > 1e-8.
+// counts[0] += tets with |det F_sl3 - 1| > 1e-8, counts[1] += tets whose
+// state is not finite.
 void launch_element_states(const MeshDev& m, const double* u, double nu, double* F,
-                           double* stress, unsigned* violations, unsigned* status,
-                           cudaStream_t s);
+                           double* stress, unsigned* counts, cudaStream_t s);
 // one warp waits (bounded by the limit that travels with status) for *flag
 // to reach epoch 1; nothing sets it, so the wait times out
 void launch_wait_probe(const unsigned* flag, unsigned* status, cudaStream_t s);

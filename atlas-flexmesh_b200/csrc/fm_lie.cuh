@@ -19,7 +19,19 @@
 // exp, log2, cbrt and sqrt are CUDA's own.
 #pragma once
 
+#include <math.h>
+
 #include <cuda_runtime.h>
+
+// device code; also host code so that a CPU build can check it against the
+// oracle's restatement
+#ifdef __CUDACC__
+#define FM_LIE_FN __host__ __device__ __forceinline__
+#define FM_LIE_NOINLINE __host__ __device__ __noinline__
+#else
+#define FM_LIE_FN inline
+#define FM_LIE_NOINLINE inline
+#endif
 
 namespace fm {
 namespace lie {
@@ -28,38 +40,38 @@ struct M3 {
     double a[9];
 };
 
-__device__ __forceinline__ M3 ident() {
+FM_LIE_FN M3 ident() {
     M3 r;
 #pragma unroll
     for (int i = 0; i < 9; ++i) r.a[i] = (i % 4 == 0) ? 1.0 : 0.0;
     return r;
 }
-__device__ __forceinline__ M3 zero() {
+FM_LIE_FN M3 zero() {
     M3 r;
 #pragma unroll
     for (int i = 0; i < 9; ++i) r.a[i] = 0.0;
     return r;
 }
-__device__ __forceinline__ M3 add(const M3& A, const M3& B) {
+FM_LIE_FN M3 add(const M3& A, const M3& B) {
     M3 r;
 #pragma unroll
     for (int i = 0; i < 9; ++i) r.a[i] = A.a[i] + B.a[i];
     return r;
 }
-__device__ __forceinline__ M3 sub(const M3& A, const M3& B) {
+FM_LIE_FN M3 sub(const M3& A, const M3& B) {
     M3 r;
 #pragma unroll
     for (int i = 0; i < 9; ++i) r.a[i] = A.a[i] - B.a[i];
     return r;
 }
-__device__ __forceinline__ M3 scale(const M3& A, double s) {
+FM_LIE_FN M3 scale(const M3& A, double s) {
     M3 r;
 #pragma unroll
     for (int i = 0; i < 9; ++i) r.a[i] = A.a[i] * s;
     return r;
 }
 // C = A B, column-major: C(r,c) = sum_k A(r,k) B(k,c)
-__device__ __forceinline__ M3 mul(const M3& A, const M3& B) {
+FM_LIE_FN M3 mul(const M3& A, const M3& B) {
     M3 C;
 #pragma unroll
     for (int c = 0; c < 3; ++c)
@@ -69,35 +81,35 @@ __device__ __forceinline__ M3 mul(const M3& A, const M3& B) {
                 A.a[r] * B.a[3 * c] + A.a[3 + r] * B.a[3 * c + 1] + A.a[6 + r] * B.a[3 * c + 2];
     return C;
 }
-__device__ __forceinline__ double trace(const M3& A) { return A.a[0] + A.a[4] + A.a[8]; }
-__device__ __forceinline__ double frob_sq(const M3& A) {
+FM_LIE_FN double trace(const M3& A) { return A.a[0] + A.a[4] + A.a[8]; }
+FM_LIE_FN double frob_sq(const M3& A) {
     double s = 0.0;
 #pragma unroll
     for (int i = 0; i < 9; ++i) s += A.a[i] * A.a[i];
     return s;
 }
-__device__ __forceinline__ double frob(const M3& A) { return sqrt(frob_sq(A)); }
+FM_LIE_FN double frob(const M3& A) { return sqrt(frob_sq(A)); }
 // max row sum / max column sum of |a| in the column-major layout
-__device__ __forceinline__ double inf_norm(const M3& A) {
+FM_LIE_FN double inf_norm(const M3& A) {
     double m = 0.0;
 #pragma unroll
     for (int r = 0; r < 3; ++r) m = fmax(m, fabs(A.a[r]) + fabs(A.a[3 + r]) + fabs(A.a[6 + r]));
     return m;
 }
-__device__ __forceinline__ double one_norm(const M3& A) {
+FM_LIE_FN double one_norm(const M3& A) {
     double m = 0.0;
 #pragma unroll
     for (int c = 0; c < 3; ++c)
         m = fmax(m, fabs(A.a[3 * c]) + fabs(A.a[3 * c + 1]) + fabs(A.a[3 * c + 2]));
     return m;
 }
-__device__ __forceinline__ double det(const M3& A) {
+FM_LIE_FN double det(const M3& A) {
     return A.a[0] * (A.a[4] * A.a[8] - A.a[7] * A.a[5]) -
            A.a[3] * (A.a[1] * A.a[8] - A.a[7] * A.a[2]) +
            A.a[6] * (A.a[1] * A.a[5] - A.a[4] * A.a[2]);
 }
 // cofactor inverse; |det| < 1e-15 gives the identity (the reference's guard)
-__device__ __forceinline__ M3 inv(const M3& A) {
+FM_LIE_FN M3 inv(const M3& A) {
     const double a00 = A.a[0], a10 = A.a[1], a20 = A.a[2];
     const double a01 = A.a[3], a11 = A.a[4], a21 = A.a[5];
     const double a02 = A.a[6], a12 = A.a[7], a22 = A.a[8];
@@ -122,12 +134,12 @@ __device__ __forceinline__ M3 inv(const M3& A) {
     r.a[8] = c22 * id;
     return r;
 }
-__device__ __forceinline__ double cond_estimate(const M3& A) {
+FM_LIE_FN double cond_estimate(const M3& A) {
     if (fabs(det(A)) < 1.0e-15) return 1.0e18;
     return fmin(one_norm(A) * one_norm(inv(A)), 1.0e18);
 }
 
-__device__ __noinline__ M3 expm(const M3& A) {
+FM_LIE_NOINLINE M3 expm(const M3& A) {
     constexpr double b1 = 0.5, b2 = 0.1, b3 = 1.0 / 120.0;
     constexpr double theta3 = 1.495585217958292;
     const double nrm = inf_norm(A);
@@ -150,7 +162,7 @@ __device__ __noinline__ M3 expm(const M3& A) {
     return R;
 }
 
-__device__ __noinline__ M3 sqrtm_db(const M3& A) {
+FM_LIE_NOINLINE M3 sqrtm_db(const M3& A) {
     M3 Y = A, Z = ident();
     for (int it = 0; it < 20; ++it) {
         if (frob(sub(mul(Y, Y), A)) < 4.0e-16) break;
@@ -163,7 +175,7 @@ __device__ __noinline__ M3 sqrtm_db(const M3& A) {
     return Y;
 }
 
-__device__ __noinline__ M3 logm(const M3& A) {
+FM_LIE_NOINLINE M3 logm(const M3& A) {
     if (!isfinite(frob_sq(A))) return zero();
     const M3 I = ident();
     {
@@ -210,7 +222,7 @@ __device__ __noinline__ M3 logm(const M3& A) {
 }
 
 // exp(log G + V) with V = 0, rescaled to det 1
-__device__ __forceinline__ M3 sl3_retraction(const M3& G) {
+FM_LIE_FN M3 sl3_retraction(const M3& G) {
     M3 R = expm(add(logm(G), zero()));
     const double d = det(R);
     if (fabs(d) > 1.0e-15) R = scale(R, 1.0 / cbrt(d));

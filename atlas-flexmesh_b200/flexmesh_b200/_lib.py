@@ -190,7 +190,7 @@ def lib() -> C.CDLL:
             "fm_newton_history": [_vp, _P(NewtonRecord), _i32, _P(_i32)],
             "fm_newton_step_cfg_host": [_vp, _vp, _f64, _P(NewtonConfig), _P(NewtonResult)],
             "fm_newton_solve_cfg": [_vp, _vp, _i32, _i32, _P(NewtonConfig), _P(NewtonResult)],
-            "fm_element_states": [_vp, _vp, _vp, _vp, _P(_u32)],
+            "fm_element_states": [_vp, _vp, _vp, _vp, _P(_u32), _P(_u32)],
             "fm_set_state_output": [_vp, _vp, _vp],
             "fm_checkpoint_save": [C.c_char_p, _P(Checkpoint)],
             "fm_checkpoint_header": [C.c_char_p, _P(Checkpoint)],
@@ -532,19 +532,21 @@ class Context:
             self._check(st, "fm_newton_solve_cfg")
         return out
 
-    def element_states(self, u, F=None, stress=None):
+    def element_states(self, u, F=None, stress=None, counts=False):
         """fm_element_states: (F_sl3 [E, 9], stress [E, 6], det violations);
-        F/stress default to ElementState's initial values (identity, zero)"""
+        with counts=True the last item is (det violations, non-finite
+        states).  F/stress default to ElementState's initial values
+        (identity, zero)"""
         t = self.torch
         if F is None:
             F = t.eye(3, dtype=t.float64, device=f"cuda:{self.device}").reshape(1, 9).repeat(
                 self.n_elems, 1).contiguous()
         if stress is None:
             stress = self._zeros(6 * self.n_elems).view(self.n_elems, 6)
-        v = _u32()
-        self._check(lib().fm_element_states(self._h, _dp(u), _dp(F), _dp(stress), C.byref(v)),
-                    "fm_element_states")
-        return F, stress, v.value
+        v, nf = _u32(), _u32()
+        self._check(lib().fm_element_states(self._h, _dp(u), _dp(F), _dp(stress), C.byref(v),
+                                            C.byref(nf)), "fm_element_states")
+        return F, stress, ((v.value, nf.value) if counts else v.value)
 
     def set_state_output(self, F=None, stress=None):
         self._state_keep = (F, stress)  # the library holds the raw pointers

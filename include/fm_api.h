@@ -412,9 +412,13 @@ fm_status fm_newton_solve(fm_ctx* ctx, double* u_dev, int first_step, int n_load
  * (initialize them as ElementState::initialize does: F = I, stress = 0).
  * det_violations (nullable): tets with |det F_sl3 - 1| > 1e-8, the count of
  * RuntimeInvariantMonitor::check_sl3_element (CORE/lie_operator.hpp:244).
- * The engine's J2 return after it (:2109) is an empty stub and not run. */
+ * nonfinite (nullable): tets whose state is not finite (under node jitter
+ * the split's sliver tets have a tiny nonzero reference Jacobian; the
+ * reference updates them too and their F can overflow).  Neither count is
+ * an error.  The engine's J2 return after it (:2109) is an empty stub and
+ * not run. */
 fm_status fm_element_states(fm_ctx* ctx, const double* u_dev, double* F_dev, double* stress_dev,
-                            uint32_t* det_violations);
+                            uint32_t* det_violations, uint32_t* nonfinite);
 /* Attach state arrays to the Newton calls: with both non-NULL every
  * fm_newton_step(_cfg) / fm_newton_solve(_cfg) updates them after each
  * update of u (the predictor's and every Newton iteration's), as the
