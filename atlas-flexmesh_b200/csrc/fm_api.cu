@@ -103,11 +103,6 @@ struct fm_ctx {
     DevBuf<double> ke_scratch;
     DevBuf<unsigned char> elem_rec;  // assembly element-pass records
     DevBuf<uint32_t> inc_pos, nbr_members;  // node-pass scatter structure
-    // pipelined assembly plan (tasks, node order, per-chunk task counts, counters)
-    DevBuf<uint4> pipe_tasks;
-    DevBuf<uint32_t> pipe_order, pipe_entasks, pipe_nntasks;
-    DevBuf<unsigned> pipe_counters;
-    fm::AsmPipe pipe[2];
 
     // solver state
     Work<double> w64;
@@ -293,8 +288,6 @@ fm::MeshDev mesh_view(const fm_ctx* c) {
     m.elem_rec = c->elem_rec.p;
     m.inc_pos = c->inc_pos.p;
     m.nbr_members = c->nbr_members.p;
-    m.pipe[0] = c->pipe[0];
-    m.pipe[1] = c->pipe[1];
     return m;
 }
 
@@ -637,41 +630,6 @@ fm_status ensure_dof_levels(fm_ctx* c) {
     return FM_OK;
 }
 
-// Plan of the pipelined assembly (fm_kernels.hpp AsmPipe): element chunks
-// of 2^14 tets, whose records (3.7 MB FP64) and ring stay in L2.  The
-// default; FM_ASM_PATH=split keeps the element and node passes as two
-// launches.
-fm_status setup_assemble_pipe(fm_ctx* c) {
-    c->pipe[0] = c->pipe[1] = fm::AsmPipe();
-    const char* path = getenv("FM_ASM_PATH");
-    if (path && std::strcmp(path, "split") == 0) return FM_OK;
-    constexpr uint32_t kShift = 14;
-    fm::AsmPipePlan plan;
-    CK(fm::plan_assemble_pipe(c->nn, c->ne, c->inc_ptr.p, c->inc_e.p, kShift, plan, c->stream));
-    if (plan.tasks.empty()) return FM_OK;
-    CK(upload(c->pipe_tasks, plan.tasks.data(), plan.tasks.size(), c->stream));
-    CK(upload(c->pipe_order, plan.node_order.data(), plan.node_order.size(), c->stream));
-    CK(upload(c->pipe_entasks, plan.elem_ntasks.data(), plan.elem_ntasks.size(), c->stream));
-    CK(upload(c->pipe_nntasks, plan.node_ntasks.data(), plan.node_ntasks.size(), c->stream));
-    CK(c->pipe_counters.reserve(1 + 2 * (size_t)plan.n_chunks));
-    for (int k = 0; k < 2; ++k) {
-        fm::AsmPipe& P = c->pipe[k];
-        P.tasks = c->pipe_tasks.p;
-        P.n_tasks = (uint32_t)plan.tasks.size();
-        P.node_order = c->pipe_order.p;
-        P.elem_ntasks = c->pipe_entasks.p;
-        P.node_ntasks = c->pipe_nntasks.p;
-        P.n_chunks = plan.n_chunks;
-        P.shift = kShift;
-        P.slots = plan.slots;
-        P.span = plan.span;
-        P.counters = c->pipe_counters.p;
-        P.grid = fm::assemble_pipe_grid(c->device, k == 1);
-    }
-    CK(cudaStreamSynchronize(c->stream));
-    return FM_OK;
-}
-
 // element -> CSR slot maps on the device (chunks of 2^20 tets through a
 // scratch buffer): into host memory, or into a device buffer
 fm_status slot_map_device(fm_ctx* c, int reference, int32_t* host_out, DevBuf<int32_t>* dev_out) {
@@ -897,7 +855,6 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
         for (size_t l = 0; l + 1 < c->node_up.size(); ++l)
             c->width_bwd = std::max(c->width_bwd, c->node_up[l + 1] - c->node_up[l]);
         TRY(setup_push_solves(c, c->node_lp, c->node_lo, c->node_up, c->node_uo));
-        TRY(setup_assemble_pipe(c));
         CK(cudaStreamSynchronize(c->stream));
         CK(c->done.reserve(std::max<size_t>(c->done.n, (size_t)c->nn + 1)));
         CK(cudaMemsetAsync(c->done.p, 0, c->done.n * sizeof(unsigned), c->stream));
@@ -1301,6 +1258,7 @@ fm_status fm_newton_config_default(fm_newton_config* g) {
     g->diverge_growth = 10.0;
     g->precision = FM_FP64;
     g->ilu_every = 1;
+    g->initial_guess = 0;
     return FM_OK;
 }
 
@@ -1336,18 +1294,45 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
     // ILU(0) of the eliminated tangent, PCG on R (norm rnorm) to itol, then
     // either u += du or du kept in `du` (FP64) for the line search.
     int n_solve = 0;
-    auto solve = [&](double rnorm, double itol, bool keep, int* its) -> fm_status {
+    bool have_prev = false;  // w32.x holds the previous Newton correction / ||R||
+    auto solve = [&](double rnorm, double itol, bool keep, int* its, bool newton) -> fm_status {
         const bool refactor = n_solve++ % g->ilu_every == 0;
         if (mixed) {
             // FP32 tangent/ILU(0)/PCG on R/||R||; the step is rescaled in FP64
             if (refactor) TRY(ilu_core<float>(c, c->fem, c->w32.K.p, c->w32.LU.p, c->w32.diag.p));
-            { PROF(FM_PROF_VECTOR, 1); fm::launch_to_f32_scaled(c->n, R, 1.0 / rnorm, c->w32.b.p, c->w32.x.p, c->stream); }
+            const bool guess = g->initial_guess && newton && have_prev;
+            { PROF(FM_PROF_VECTOR, 1); fm::launch_to_f32_scaled(c->n, R, 1.0 / rnorm, c->w32.b.p, guess ? nullptr : c->w32.x.p, c->stream); }
+            if (guess) {
+                // x0 = gamma x_prev with gamma = x_prev.b / x_prev.K x_prev: the
+                // energy-norm projection of the solution on the previous
+                // correction (corrections of a linearly converging Newton
+                // iteration are nearly parallel); never worse than x0 = 0
+                float* part = reinterpret_cast<float*>(c->partials.p);
+                {
+                    PROF(FM_PROF_SPMV, 1);
+                    fm::launch_spmv_nodes<float>(c->nn, c->nbr_ptr.p, c->nbr.p, c->w32.K.p,
+                                                 c->w32.x.p, c->w32.Ap.p, nullptr, nullptr,
+                                                 nullptr, c->stream);
+                }
+                {
+                    PROF(FM_PROF_VECTOR, 2);
+                    fm::launch_dot<float>(c->n, c->w32.x.p, c->w32.b.p, part, c->counter(),
+                                          &c->sc.p->guess_xb, c->stream);
+                    fm::launch_dot<float>(c->n, c->w32.x.p, c->w32.Ap.p, part, c->counter(),
+                                          &c->sc.p->guess_xkx, c->stream);
+                }
+                TRY(sync_scalars(c));
+                const double xkx = c->h_sc->guess_xkx;
+                const double gam = xkx > 0.0 && std::isfinite(xkx) ? c->h_sc->guess_xb / xkx : 0.0;
+                { PROF(FM_PROF_VECTOR, 1); fm::launch_scale_f32(c->n, c->w32.x.p, (float)gam, c->stream); }
+            }
             Op<float> A{c, &c->fem, true, c->w32.K.p, c->w32.LU.p, c->w32.diag.p, c->w32.t.p,
                         c->grid_trsv32, c->w32.dinv.p};
             TRY(pcg_core<float>(c, A, c->n, c->w32.b.p, c->w32.x.p, itol, g->max_pcg, its,
                                 nullptr));
             if (keep) { PROF(FM_PROF_VECTOR, 1); fm::launch_f32_to_f64_scaled(c->n, c->w32.x.p, rnorm, du, c->stream); }
             else { PROF(FM_PROF_VECTOR, 1); fm::launch_axpy_u_f32(c->n, c->w32.x.p, rnorm, u, c->stream); }
+            have_prev = newton;
         } else {
             if (refactor) TRY(ilu_core<double>(c, c->fem, c->w64.K.p, c->w64.LU.p, c->w64.diag.p));
             CK(cudaMemsetAsync(du, 0, sizeof(double) * c->n, c->stream));
@@ -1416,7 +1401,7 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
             have_r0 = true;
             int its = 0;
             const double ptol = g->predictor_tol > 0.0 ? g->predictor_tol : tol;
-            if (r0 > 0.0) TRY(solve(r0, ptol, false, &its));
+            if (r0 > 0.0) TRY(solve(r0, ptol, false, &its, false));
             n_pcg += its;
             ++n_newton;
             record(0, its, r0, 1.0, ptol);
@@ -1471,7 +1456,7 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
             rn > (g->diverge_rate > 0.0 ? g->diverge_rate : 0.9) * r_prev)
             tol = std::max(g->inner_tol_min, 0.1 * tol);
         int its = 0;
-        TRY(solve(rn, tol, keep_du, &its));
+        TRY(solve(rn, tol, keep_du, &its, true));
         double alpha = 1.0;
         if (keep_du) {
             // Armijo backtracking on ||R|| with residual-only re-assembly at

@@ -34,6 +34,7 @@ struct DevScalars {
     double relres;   // sqrt(rz_new / max(b.b, 1e-300))
     double norm2;    // generic reduction output
     double scale;    // rhs scaling for the FP32 inner solve
+    double guess_xb, guess_xkx;  // x_prev . b and x_prev . K x_prev (initial guess)
     unsigned stop;   // 1: |pAp| < 1e-60 breakdown
     unsigned status; // FM_FLAG_* bits
     unsigned wait_budget;  // bounded-wait limit in 1024 cycles (0: kWaitCycles); follows status

@@ -178,31 +178,12 @@ __global__ void __launch_bounds__(128, 4)
     if (flags) raise_flag(status, flags);
 }
 
-// Where element e's record lives: rec + e, or, for the pipelined assembly,
-// in a ring of `slots` chunks of 2^shift records (chunk c in slot c % slots).
-struct RecRing {
-    uint32_t shift = 31, slots = 0;  // slots == 0: no ring
-    __device__ __forceinline__ size_t index(uint32_t e) const {
-        if (!slots) return e;
-        const uint32_t c = e >> shift;
-        return ((size_t)(c % slots) << shift) | (e & ((1u << shift) - 1u));
-    }
-};
-
-// a record field: a plain load, or an L2 load (records written during the
-// same kernel by other SMs must not come from a stale L1 line)
-template <bool kL2, typename T>
-__device__ __forceinline__ T rec_ld(const T* p) {
-    if constexpr (kL2) return __ldcg(p);
-    else return *p;
-}
-
 // Node pass for one node: one warp owns it.  Lane l < mi stages incident
 // tet l's record (gradients, the owner's vertex force, tangent scalars) in
 // shared memory; lane k then forms block (n, nbr[k]).
-template <typename KT, bool kL2>
+template <typename KT>
 __device__ __forceinline__ void asm_node(const MeshDev& m, const ElemRec<KT>* __restrict__ rec,
-                                         RecRing ring, uint32_t n, KT* __restrict__ K,
+                                         uint32_t n, KT* __restrict__ K,
                                          double* __restrict__ f, double* __restrict__ R,
                                          int apply_bc, AsmStage<KT>& S, int lane) {
 
@@ -220,25 +201,25 @@ __device__ __forceinline__ void asm_node(const MeshDev& m, const ElemRec<KT>* __
     if (lane < mi) {
         const uint32_t e = __ldg(m.inc + e0 + lane);
         packed = __ldg(m.inc_pos + e0 + lane);
-        const ElemRec<KT>& r = rec[ring.index(e)];
-        const bool act = rec_ld<kL2>(&r.active) != KT(0);
+        const ElemRec<KT>& r = rec[e];
+        const bool act = r.active != KT(0);
         if (act) {
             const int il = byte_index(packed, (uint32_t)self_k);
-            fi0 = rec_ld<kL2>(&r.f[3 * il]);
-            fi1 = rec_ld<kL2>(&r.f[3 * il + 1]);
-            fi2 = rec_ld<kL2>(&r.f[3 * il + 2]);
+            fi0 = r.f[3 * il];
+            fi1 = r.f[3 * il + 1];
+            fi2 = r.f[3 * il + 2];
         }
         if (K != nullptr) {
             // an inactive tet (degenerate at this state) stays in the edge
             // lists with zero data: it adds exact zeros
 #pragma unroll
-            for (int q = 0; q < 12; ++q) S.d[lane][q] = act ? rec_ld<kL2>(&r.d[q]) : KT(0);
+            for (int q = 0; q < 12; ++q) S.d[lane][q] = act ? r.d[q] : KT(0);
             S.fI[lane][0] = (KT)fi0;
             S.fI[lane][1] = (KT)fi1;
             S.fI[lane][2] = (KT)fi2;
-            S.vabm[lane][0] = act ? rec_ld<kL2>(&r.s[0]) : KT(0);
-            S.vabm[lane][1] = act ? rec_ld<kL2>(&r.s[1]) : KT(0);
-            S.vabm[lane][2] = act ? rec_ld<kL2>(&r.s[2]) : KT(0);
+            S.vabm[lane][0] = act ? r.s[0] : KT(0);
+            S.vabm[lane][1] = act ? r.s[1] : KT(0);
+            S.vabm[lane][2] = act ? r.s[2] : KT(0);
         }
     }
     S.pos[lane] = packed;
@@ -322,94 +303,7 @@ __global__ void __launch_bounds__(kAsmWarps * 32, 3)
     const int wi = threadIdx.x >> 5;
     const uint32_t n = blockIdx.x * kAsmWarps + wi;
     if (n >= m.n_nodes) return;  // uniform per warp
-    asm_node<KT, false>(m, rec, RecRing{}, n, K, f, R, apply_bc, stage[wi], lane);
-}
-
-// Bounded wait until *cnt reaches target (acquire); FM_FLAG_TIMEOUT on expiry.
-__device__ __forceinline__ void wait_count(const unsigned* cnt, unsigned target,
-                                           unsigned* status) {
-    if (ld_acquire(cnt) >= target) return;
-    const long long t0 = clock64(), limit = wait_limit(status);
-    for (unsigned it = 1;; ++it) {
-        if (ld_acquire(cnt) >= target) return;
-        if ((it & 31u) == 0) {
-            if (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) return;
-            if (clock64() - t0 > limit) {
-                raise_flag(status, FM_FLAG_TIMEOUT);
-                return;
-            }
-        }
-    }
-}
-
-constexpr int kPipeThreads = kAsmWarps * 32;
-
-// The pipelined assembly: see AsmPipe.  Thread 0 draws a ticket and waits
-// for the task's inputs; the block runs the task; every thread fences its
-// writes before thread 0 counts the task done.
-template <typename KT>
-__global__ void __launch_bounds__(kPipeThreads, 2)
-    k_assemble_pipe(MeshDev m, AsmPipe P, const double* __restrict__ u,
-                    ElemRec<KT>* __restrict__ rec, KT* __restrict__ K, double* __restrict__ f,
-                    double* __restrict__ R, int apply_bc, unsigned* __restrict__ status) {
-    __shared__ AsmStage<KT> stage[kAsmWarps];
-    __shared__ uint4 task_s;
-    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
-    const RecRing ring{P.shift, P.slots};
-    unsigned* const ticket = P.counters;
-    unsigned* const edone = P.counters + 1;
-    unsigned* const ndone = P.counters + 1 + P.n_chunks;
-    unsigned flags = 0;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            const unsigned t = atomicAdd(ticket, 1u);
-            uint4 tk = t < P.n_tasks ? P.tasks[t] : make_uint4(~0u, 0u, 0u, 0u);
-            if (tk.x != ~0u) {
-                const uint32_t c = tk.x & 0x7fffffffu;
-                if (tk.x >> 31) {
-                    for (uint32_t cc = c > P.span ? c - P.span : 0; cc <= c; ++cc)
-                        wait_count(edone + cc, P.elem_ntasks[cc], status);
-                } else if (P.slots && c >= P.slots) {
-                    for (uint32_t cc = c - P.slots; cc + 2 <= c; ++cc)
-                        wait_count(ndone + cc, P.node_ntasks[cc], status);
-                }
-                __threadfence();
-            }
-            task_s = tk;
-        }
-        __syncthreads();
-        const uint4 tk = task_s;
-        __syncthreads();  // task_s is rewritten only after every thread read it
-        if (tk.x == ~0u) break;
-        const bool node = (tk.x >> 31) != 0;
-        if (!node) {
-            for (uint32_t e = tk.y + threadIdx.x; e < tk.z; e += blockDim.x)
-                flags |= asm_element<KT>(m, u, e, rec + ring.index(e), K != nullptr);
-        } else {
-            for (uint32_t q = tk.y + (uint32_t)wi; q < tk.z; q += kAsmWarps)
-                asm_node<KT, true>(m, rec, ring, __ldg(P.node_order + q), K, f, R, apply_bc,
-                                   stage[wi], lane);
-        }
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0) atomicAdd((node ? ndone : edone) + (tk.x & 0x7fffffffu), 1u);
-    }
-    if (flags) raise_flag(status, flags);
-}
-
-int assemble_pipe_grid(int device, bool fp32) {
-    int per_sm = 0, sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    const cudaError_t e =
-        fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_assemble_pipe<float>,
-                                                             kPipeThreads, 0)
-             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_assemble_pipe<double>,
-                                                             kPipeThreads, 0);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    return per_sm * sms;
+    asm_node<KT>(m, rec, n, K, f, R, apply_bc, stage[wi], lane);
 }
 
 template <typename KT>
@@ -417,15 +311,6 @@ static void launch_assemble_t(const MeshDev& m, const double* u, KT* K, double* 
                               int apply_bc, unsigned* status, cudaStream_t s) {
     if (m.n_nodes == 0) return;
     ElemRec<KT>* rec = static_cast<ElemRec<KT>*>(m.elem_rec);
-    const AsmPipe* pipe = &m.pipe[sizeof(KT) == 4 ? 1 : 0];
-    if (pipe->n_tasks && pipe->grid > 0) {
-        cudaMemsetAsync(pipe->counters, 0, sizeof(unsigned) * (1 + 2 * (size_t)pipe->n_chunks),
-                        s);
-        const unsigned grid = std::min<unsigned>((unsigned)pipe->grid, pipe->n_tasks);
-        k_assemble_pipe<KT><<<grid, kPipeThreads, 0, s>>>(m, *pipe, u, rec, K, f, R, apply_bc,
-                                                          status);
-        return;
-    }
     if (m.n_elems) {
         unsigned ge = (m.n_elems + 127) / 128;
         if (ge > 148u * 32u) ge = 148u * 32u;
@@ -965,8 +850,17 @@ __global__ void k_to_f32_scaled(uint32_t n, const double* __restrict__ R, double
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += gridDim.x * blockDim.x) {
         b32[i] = (float)(R[i] * inv_scale);
-        x32[i] = 0.0f;
+        if (x32) x32[i] = 0.0f;
     }
+}
+
+__global__ void k_scale_f32(uint32_t n, float* __restrict__ x, float g) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x)
+        x[i] *= g;
+}
+void launch_scale_f32(uint32_t n, float* x, float g, cudaStream_t s) {
+    k_scale_f32<<<kRedBlocks * 2, kVecThreads, 0, s>>>(n, x, g);
 }
 void launch_to_f32_scaled(uint32_t n, const double* R, double inv_scale, float* b32, float* x32,
                           cudaStream_t s) {

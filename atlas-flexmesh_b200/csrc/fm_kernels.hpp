@@ -8,26 +8,6 @@
 
 namespace fm {
 
-// Plan of the pipelined assembly (one launch): the element pass and the node
-// pass run as interleaved tasks handed out by ticket, E(0), N(0), E(1), ...
-// E(c) evaluates element chunk c (2^shift tets) into a record ring of
-// `slots` chunks (0: no ring, records at their element index); N(c) runs the
-// node pass of the nodes whose last incident tet lies in chunk c.  A node
-// task waits for element chunks c - span .. c (span: the most chunks a
-// node's incident tets spread over, minus one); an element task whose ring
-// slot is in use waits for the node chunks that read it.  Every wait is on
-// a task with an earlier ticket, bounded by the status word's limit.
-struct AsmPipe {
-    const uint4* tasks = nullptr;          // {node << 31 | chunk, begin, end, 0}
-    uint32_t n_tasks = 0;
-    const uint32_t* node_order = nullptr;  // node positions of the node tasks
-    const uint32_t* elem_ntasks = nullptr; // tasks per chunk
-    const uint32_t* node_ntasks = nullptr;
-    uint32_t n_chunks = 0, shift = 14, slots = 0, span = 0;
-    unsigned* counters = nullptr;          // [0] ticket, [1 + c] element, [1 + Q + c] node
-    int grid = 0;
-};
-
 // Mesh/material data resident on the device (read by assembly kernels).
 struct MeshDev {
     uint32_t n_nodes = 0, n_elems = 0;
@@ -53,9 +33,6 @@ struct MeshDev {
     // l-th incident tet (not skipped) holds the edge to neighbour entry j
     const uint32_t* inc_pos = nullptr;
     const uint32_t* nbr_members = nullptr;
-    // pipelined assembly plans, FP64 [0] and FP32 tangent [1] (n_tasks == 0:
-    // the two-launch form)
-    AsmPipe pipe[2];
 };
 constexpr size_t kElemRecBytes = 224;
 
@@ -65,13 +42,10 @@ constexpr size_t kElemRecBytes = 224;
 // node-owner pass that writes every CSR row block once.  K (double or float,
 // may be null for a residual-only call), f (FP64, may be null), R = -f with
 // zeros on constrained DOFs (may be null).  m.elem_rec is required.
-// The pipelined single launch where m.pipe has a plan, else two launches.
 void launch_assemble(const MeshDev& m, const double* u, double* K, double* f, double* R,
                      int apply_bc, unsigned* status, cudaStream_t s);
 void launch_assemble(const MeshDev& m, const double* u, float* K, double* f, double* R,
                      int apply_bc, unsigned* status, cudaStream_t s);
-// resident blocks of the pipelined assembly kernel on this device
-int assemble_pipe_grid(int device, bool fp32);
 // Element-centric scatter through an int32 slot map (reference pattern).
 // K and f must be zeroed by the caller; Ke_scratch holds 144*n_elems doubles.
 void launch_assemble_slotmap(const MeshDev& m, const double* u, const int32_t* slot, double* K,
@@ -149,9 +123,11 @@ void launch_set_bc_values(uint32_t n, const uint8_t* mask, const double* val, do
 // free-DOF squared norm of R into *out
 void launch_norm2(uint32_t n, const double* R, double* partials, unsigned* counter, double* out,
                   cudaStream_t s);
-// b32 = R * inv_scale (FP32), x32 = 0
+// b32 = R * inv_scale (FP32), x32 = 0 (x32 nullable)
 void launch_to_f32_scaled(uint32_t n, const double* R, double inv_scale, float* b32, float* x32,
                           cudaStream_t s);
+// x *= g (FP32)
+void launch_scale_f32(uint32_t n, float* x, float g, cudaStream_t s);
 // u += du (FP64)
 void launch_axpy_u(uint32_t n, const double* du, double* u, cudaStream_t s);
 // u += scale * du32

@@ -473,63 +473,6 @@ __global__ void k_slot_map(uint32_t e0, uint32_t count, const uint4* __restrict_
 
 }  // namespace
 
-namespace {
-// first and last incident chunk of every node (0, 0 without incident tets)
-__global__ void k_node_chunks(uint32_t nn, const uint32_t* __restrict__ inc_ptr,
-                              const uint32_t* __restrict__ inc_e, uint32_t shift, uint32_t* lo,
-                              uint32_t* hi) {
-    for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += gridDim.x * blockDim.x) {
-        const uint32_t b = inc_ptr[n], e = inc_ptr[n + 1];
-        lo[n] = b < e ? inc_e[b] >> shift : 0u;
-        hi[n] = b < e ? inc_e[e - 1] >> shift : 0u;
-    }
-}
-}  // namespace
-
-cudaError_t plan_assemble_pipe(uint32_t nn, uint32_t ne, const uint32_t* inc_ptr,
-                               const uint32_t* inc_e, uint32_t shift, AsmPipePlan& plan,
-                               cudaStream_t s) {
-    plan = AsmPipePlan();
-    if (!nn || !ne) return cudaSuccess;
-    DevBuf<uint32_t> lo_d, hi_d;
-    SCK(lo_d.reserve(nn));
-    SCK(hi_d.reserve(nn));
-    k_node_chunks<<<blocks_for(nn, 256), 256, 0, s>>>(nn, inc_ptr, inc_e, shift, lo_d.p, hi_d.p);
-    std::vector<uint32_t> lo, hi;
-    SCK(down(lo, lo_d.p, nn, s));
-    SCK(down(hi, hi_d.p, nn, s));
-    SCK(cudaStreamSynchronize(s));
-    const uint32_t Q = (uint32_t)(((uint64_t)ne + (1ull << shift) - 1) >> shift);
-    plan.n_chunks = Q;
-    std::vector<uint32_t> cnt(Q + 1, 0);
-    for (uint32_t n = 0; n < nn; ++n) {
-        plan.span = std::max(plan.span, hi[n] - lo[n]);
-        cnt[hi[n] + 1]++;
-    }
-    for (uint32_t c = 0; c < Q; ++c) cnt[c + 1] += cnt[c];
-    plan.node_order.resize(nn);
-    {
-        std::vector<uint32_t> fill(cnt.begin(), cnt.end() - 1);
-        for (uint32_t n = 0; n < nn; ++n) plan.node_order[fill[hi[n]]++] = n;
-    }
-    plan.slots = plan.span + 2 < Q ? plan.span + 2 : 0;
-    plan.elem_ntasks.assign(Q, 0);
-    plan.node_ntasks.assign(Q, 0);
-    for (uint32_t c = 0; c < Q; ++c) {
-        const uint32_t e0 = c << shift, e1 = std::min<uint64_t>((uint64_t)(c + 1) << shift, ne);
-        for (uint32_t e = e0; e < e1; e += kPipeElemTask) {
-            plan.tasks.push_back(make_uint4(c, e, std::min(e + kPipeElemTask, e1), 0));
-            plan.elem_ntasks[c]++;
-        }
-        for (uint32_t q = cnt[c]; q < cnt[c + 1]; q += kPipeNodeTask) {
-            plan.tasks.push_back(
-                make_uint4(0x80000000u | c, q, std::min(q + kPipeNodeTask, cnt[c + 1]), 0));
-            plan.node_ntasks[c]++;
-        }
-    }
-    return cudaSuccess;
-}
-
 void launch_slot_map(uint32_t e0, uint32_t count, const uint4* conn, const uint32_t* nbr_ptr,
                      const uint32_t* nbr, int reference, int32_t* slot, cudaStream_t s) {
     if (!count) return;

@@ -61,21 +61,6 @@ cudaError_t build_mesh_device(uint32_t n_nodes, uint32_t n_elems, const uint4* c
                               MeshSetupDev& d, MeshSetupHost& h, unsigned* status, int* result,
                               cudaStream_t s);
 
-// Plan of the pipelined assembly (fm_kernels.hpp AsmPipe) on the host:
-// element chunks of 2^shift tets, each node placed in the chunk of its last
-// incident tet (nodes of a chunk ascending), tasks of 512 tets / 64 nodes in
-// the order E(0), N(0), E(1), N(1), ..., the spread `span` and the record
-// ring's slot count (0 when the ring would hold every chunk anyway).
-struct AsmPipePlan {
-    uint32_t n_chunks = 0, span = 0, slots = 0;
-    std::vector<uint4> tasks;
-    std::vector<uint32_t> node_order, elem_ntasks, node_ntasks;
-};
-constexpr uint32_t kPipeElemTask = 512, kPipeNodeTask = 64;
-cudaError_t plan_assemble_pipe(uint32_t n_nodes, uint32_t n_elems, const uint32_t* inc_ptr,
-                               const uint32_t* inc_e, uint32_t shift, AsmPipePlan& plan,
-                               cudaStream_t s);
-
 // Element -> CSR slot map of tets e0 .. e0+count-1 (144 int32 per tet,
 // slot[(i*3+di)*12 + j*3+dj]) for the solve pattern or, reference != 0, the
 // reference's own column fill (last duplicate wins, missing -1).

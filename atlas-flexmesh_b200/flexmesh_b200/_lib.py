@@ -49,7 +49,7 @@ class NewtonConfig(C.Structure):
                 ("inner_tol_min", C.c_double), ("max_newton", C.c_int), ("max_pcg", C.c_int),
                 ("line_search", C.c_int), ("ls_c", C.c_double), ("diverge_rate", C.c_double),
                 ("diverge_count", C.c_int), ("diverge_growth", C.c_double),
-                ("precision", C.c_int), ("ilu_every", C.c_int)]
+                ("precision", C.c_int), ("ilu_every", C.c_int), ("initial_guess", C.c_int)]
 
 
 class NewtonResult(C.Structure):

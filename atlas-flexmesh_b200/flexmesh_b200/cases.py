@@ -3,6 +3,7 @@
     python -m flexmesh_b200.cases trsv     --N 64 --prec mixed --applies 4
     python -m flexmesh_b200.cases ilu      --N 64 --prec fp64 --reps 2
     python -m flexmesh_b200.cases assemble --N 128 --prec fp64 --reps 5
+    python -m flexmesh_b200.cases newton   --N 64 --levels 1 --inner-tol 0.2
     python -m flexmesh_b200.cases adjoint  --N 32 --fd 64
     python -m flexmesh_b200.cases incompressible --N 48
 
@@ -186,6 +187,34 @@ def _solve_path(ctx, n, n_steps, prec, inner_tol, rtol=1e-10, u0=None, steps=Non
     return u, newton, pcg, per_step
 
 
+def case_newton(a):
+    """Load levels 1 .. a.levels of the scale-up block in mixed precision with
+    the benchmark's Newton settings (inner PCG to 0.2, predictor to 1e-6,
+    the engine's line search), timed and broken down by kernel class: a
+    small, self-contained command for launch lists."""
+    P = configs.scaleup_block(a.N)
+    ctx = problem_context(P)
+    u = torch.zeros(P.xyz.size, dtype=torch.float64, device="cuda")
+    cfg = dict(newton_rtol=1e-10, inner_tol=a.inner_tol, predictor_tol=a.predictor_tol,
+               max_newton=400, max_pcg=20000, line_search=10, ls_c=1e-4, prec=L.FM_MIXED,
+               ilu_every=a.ilu_every, initial_guess=a.initial_guess)
+    ctx.profile_enable(True)
+    levels = []
+    with Timer(ctx.stream) as t:
+        for lvl in range(1, a.levels + 1):
+            r = ctx.newton_step_cfg(u, lvl / P.n_steps, **cfg)
+            levels.append((lvl, r["newton_iters"], r["pcg_iters"], r["backtracks"]))
+    prof = ctx.profile_read()
+    if a.save_u:
+        np.save(a.save_u, u.cpu().numpy())
+    return {"case": "newton", "N": a.N, "levels": levels, "ms": round(t.ms, 1),
+            "inner_tol": a.inner_tol, "predictor_tol": a.predictor_tol,
+            "ilu_every": a.ilu_every, "initial_guess": a.initial_guess,
+            "newton_total": sum(x[1] for x in levels), "pcg_total": sum(x[2] for x in levels),
+            "profile_ms": {k: round(v["ms"], 1) for k, v in prof.items()},
+            "launches": {k: v["kernels"] for k, v in prof.items()}}
+
+
 def case_adjoint(a):
     """Material gradients of L = 1/2 |u_top(mu) - u*|^2 on the 32^3 block:
     u* from the 'true' log-normal mu (seed A), the model mu from seed B.
@@ -342,7 +371,8 @@ def case_incompressible(a):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m flexmesh_b200.cases")
-    ap.add_argument("case", choices=["trsv", "ilu", "assemble", "adjoint", "incompressible"])
+    ap.add_argument("case", choices=["trsv", "ilu", "assemble", "newton", "adjoint",
+                                     "incompressible"])
     ap.add_argument("--N", type=int, default=None)
     ap.add_argument("--prec", choices=list(PREC), default="fp64")
     ap.add_argument("--applies", type=int, default=4)
@@ -355,13 +385,19 @@ def main(argv=None):
     ap.add_argument("--fd-step", type=float, default=1e-6)
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--max-newton", type=int, default=3000)
+    ap.add_argument("--levels", type=int, default=1)
+    ap.add_argument("--predictor-tol", type=float, default=1e-6)
+    ap.add_argument("--ilu-every", type=int, default=1)
+    ap.add_argument("--initial-guess", type=int, default=0)
+    ap.add_argument("--save-u", default=None)
     a = ap.parse_args(argv)
     if not torch.cuda.is_available():
         raise SystemExit("cases need a CUDA device")
-    default_N = {"trsv": 64, "ilu": 64, "assemble": 128, "adjoint": 32, "incompressible": 48}
+    default_N = {"trsv": 64, "ilu": 64, "assemble": 128, "newton": 64, "adjoint": 32,
+                 "incompressible": 48}
     if a.N is None:
         a.N = default_N[a.case]
-    fn = {"trsv": case_trsv, "ilu": case_ilu, "assemble": case_assemble,
+    fn = {"trsv": case_trsv, "ilu": case_ilu, "assemble": case_assemble, "newton": case_newton,
           "adjoint": case_adjoint, "incompressible": case_incompressible}[a.case]
     print(json.dumps(fn(a)), flush=True)
 

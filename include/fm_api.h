@@ -318,7 +318,8 @@ fm_status fm_newton_step_host(fm_ctx* ctx, double* u_host, double load_frac, dou
  * inner_tol 1e-12, predictor_tol 0 (= inner_tol), inner_tol_min 0 (off),
  * max_newton 200, max_pcg 5000, line_search 10 with ls_c 1e-4 (the engine's
  * armijo_line_search_true(..., line_search_c = 1e-4, 10), :2314, :2581),
- * diverge_rate 0 (off), diverge_count 3, diverge_growth 10, FP64, ilu_every 1. */
+ * diverge_rate 0 (off), diverge_count 3, diverge_growth 10, FP64, ilu_every 1,
+ * initial_guess 0. */
 typedef struct {
     double newton_rtol;    /* stop when ||R|| < newton_rtol ||R_0|| */
     double newton_atol;    /* ... or ||R|| < newton_atol */
@@ -337,6 +338,10 @@ typedef struct {
                               solve of a load step (1: every solve, as pcg_solve_ilu0
                               does; k > 1: an earlier tangent's factors precondition
                               the current tangent, which PCG still solves) */
+    int initial_guess;     /* mixed precision: 1 starts each Newton correction's PCG from
+                              gamma x_prev, the previous correction (per ||R||) scaled by
+                              the energy-norm projection gamma = x_prev.b / x_prev.K x_prev;
+                              0 starts from zero as pcg_solve_ilu0's callers do */
 } fm_newton_config;
 
 typedef struct {
