@@ -119,7 +119,8 @@ def case_trsv(a):
     return {"case": "trsv", "N": a.N, "prec": a.prec, "applies": p["calls"],
             "ms_per_apply": round(per, 4), "bytes_per_apply": B,
             "achieved_gbs": round(B / per / 1e6, 1), "peak_gbs": peak, "peak_kind": kind,
-            "frac": round(B / per / 1e6 / peak, 4), "wall_ms": round(t.ms, 2)}
+            "frac": round(B / per / 1e6 / peak, 4), "wall_ms": round(t.ms, 2),
+            "flags": ctx.flags()}
 
 
 def case_ilu(a):
