@@ -399,12 +399,12 @@ fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
     c->pu_ok32 = c->pu_ok64 = false;
     const char* path = getenv("FM_TRSV_PATH");
     if (path && std::strcmp(path, "push") != 0) return FM_OK;
+    constexpr uint32_t kCluster = 8;
     constexpr size_t kMaxSmem = 227 * 1024;
     auto env = [](const char* name, int dflt, int lo_, int hi) {
         const char* v = getenv(name);
         return v ? std::min(hi, std::max(lo_, atoi(v))) : dflt;
     };
-    const uint32_t kCluster = (uint32_t)env("FM_TRSV_PUSH_CLUSTER", 8, 1, (int)fm::kPushMax);
     const int warps32 = env("FM_TRSV_PUSH_WARPS", fm::push_max_warps(4), 1, fm::push_max_warps(4));
     const int warps64 = std::min(warps32, fm::push_max_warps(8));
     const uint32_t block = (uint32_t)env("FM_TRSV_PUSH_BLOCK", 0, 0, 1 << 20);
@@ -413,18 +413,10 @@ fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
     const int ncl = std::min(nc32, nc64);
     if (ncl < 1) return FM_OK;
     fm::PushPlan p;
-    // FM_TRSV_PUSH_CHAINS=1: chains of consecutive neighbouring nodes stay in
-    // one half-warp (push_plan_chains), laid out for the FP64 warp count,
-    // which both precisions then use
-    const bool chains = env("FM_TRSV_PUSH_CHAINS", 0, 0, 1) != 0;
-    auto plan = [&](uint32_t max_slots) {
-        return chains ? fm::push_plan_chains(c->graph, lp, lo, up, uo, (uint32_t)ncl, kCluster,
-                                             (uint32_t)warps64, max_slots, p)
-                      : fm::push_plan(c->graph, lp, lo, up, uo, (uint32_t)ncl, kCluster, block,
-                                      max_slots, p);
-    };
-    if (!plan((uint32_t)(kMaxSmem / fm::push_smem_bytes(1, 8))) &&
-        !plan((uint32_t)(kMaxSmem / fm::push_smem_bytes(1, 4))))
+    if (!fm::push_plan(c->graph, lp, lo, up, uo, (uint32_t)ncl, kCluster, block,
+                       (uint32_t)(kMaxSmem / fm::push_smem_bytes(1, 8)), p) &&
+        !fm::push_plan(c->graph, lp, lo, up, uo, (uint32_t)ncl, kCluster, block,
+                       (uint32_t)(kMaxSmem / fm::push_smem_bytes(1, 4)), p))
         return FM_OK;
     auto fits = [&](size_t vb) {
         return fm::push_smem_bytes(std::max(p.max_slot_f, p.max_slot_b), vb) <= kMaxSmem;
@@ -445,8 +437,8 @@ fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
     fm::PushSolve v;
     v.n_ctas = p.n_ctas;
     v.cluster = p.cluster;
-    v.warps32 = p.warps ? p.warps : (uint32_t)warps32;
-    v.warps64 = p.warps ? p.warps : (uint32_t)warps64;
+    v.warps32 = (uint32_t)warps32;
+    v.warps64 = (uint32_t)warps64;
     v.max_slot_f = p.max_slot_f;
     v.max_slot_b = p.max_slot_b;
     v.pos_f = c->pu_pos_f.p;

@@ -159,49 +159,6 @@ uint32_t csr_levels(uint32_t n, const uint32_t* row_ptr, const uint32_t* col_idx
     return levels_from_depth(depth, maxd, ptr, rows);
 }
 
-// The slot plan of one direction (PushPlan::src entries on that side, the
-// push lists, slot counts) for a CTA assignment cta[] and slab bounds sb
-// (slab s = nodes sb[s] .. sb[s+1]-1 on CTAs s*cluster ..).  False when a
-// CTA needs more than max_slots slots or a node has more than 16
-// neighbours on the side.
-static bool push_slots(const NodeGraph& g, const std::vector<uint32_t>& cta,
-                       const std::vector<uint32_t>& sb, uint32_t cluster, bool lower,
-                       uint32_t max_slots, PushPlan& plan) {
-    const uint32_t nn = g.n_nodes, n_clusters = (uint32_t)sb.size() - 1;
-    const uint32_t nc = n_clusters * cluster;
-    std::vector<uint32_t>& push = lower ? plan.push_f : plan.push_b;
-    std::vector<uint32_t>& nslot = lower ? plan.nslot_f : plan.nslot_b;
-    uint32_t& max_slot = lower ? plan.max_slot_f : plan.max_slot_b;
-    push.assign((size_t)nn * kPushMax, ~0u);
-    nslot.assign(nc, 0);
-    std::vector<uint8_t> npush(nn, 0);
-    for (uint32_t s = 0; s < n_clusters; ++s) {
-        const uint32_t b = sb[s], e = sb[s + 1];
-        // slot of producer m in the slab's CTA of rank r: slot[(m - b) * cluster + r]
-        std::vector<uint32_t> slot((size_t)(e - b) * cluster, ~0u);
-        for (uint32_t n = b; n < e; ++n) {
-            const uint32_t c = cta[n], r = c - s * cluster;
-            uint32_t cnt = 0;
-            for (uint32_t k = g.ptr[n]; k < g.ptr[n + 1]; ++k) {
-                const uint32_t m = g.nbr[k];
-                if (m == n || (m < n) != lower) continue;
-                ++cnt;
-                if (m < b || m >= e) continue;  // another slab: through global memory
-                uint32_t& sl = slot[(size_t)(m - b) * cluster + r];
-                if (sl == ~0u) {
-                    sl = nslot[c]++;
-                    if (sl >= max_slots) return false;
-                    push[(size_t)m * kPushMax + npush[m]++] = r << 20 | sl;
-                }
-                plan.src[k] = sl;
-            }
-            if (cnt > 16) return false;
-        }
-    }
-    max_slot = nc ? *std::max_element(nslot.begin(), nslot.end()) : 0;
-    return true;
-}
-
 bool push_plan(const NodeGraph& g, const std::vector<uint32_t>& fwd_ptr,
                const std::vector<uint32_t>& fwd_order, const std::vector<uint32_t>& bwd_ptr,
                const std::vector<uint32_t>& bwd_order, uint32_t n_clusters, uint32_t cluster,
@@ -258,14 +215,45 @@ bool push_plan(const NodeGraph& g, const std::vector<uint32_t>& fwd_ptr,
         for (uint32_t R = 16; R <= 512; R += R < 128 ? 1 : 8) cand.push_back({share(R), R});
         std::sort(cand.begin(), cand.end());
     }
-    std::vector<uint32_t> cta(nn), sb(n_clusters + 1);
-    for (uint32_t t = 0; t <= n_clusters; ++t) sb[t] = push_slab_begin(t, nn, n_clusters);
+    std::vector<uint32_t> cta(nn);
+    auto slots = [&](bool lower, std::vector<uint32_t>& push, std::vector<uint32_t>& nslot,
+                     uint32_t& max_slot) {
+        push.assign((size_t)nn * kPushMax, ~0u);
+        nslot.assign(nc, 0);
+        std::vector<uint8_t> npush(nn, 0);
+        for (uint32_t s = 0; s < n_clusters; ++s) {
+            const uint32_t b = push_slab_begin(s, nn, n_clusters);
+            const uint32_t e = push_slab_begin(s + 1, nn, n_clusters);
+            // slot of producer m in the slab's CTA of rank r: slot[(m - b) * cluster + r]
+            std::vector<uint32_t> slot((size_t)(e - b) * cluster, ~0u);
+            for (uint32_t n = b; n < e; ++n) {
+                const uint32_t c = cta[n], r = c - s * cluster;
+                uint32_t cnt = 0;
+                for (uint32_t k = g.ptr[n]; k < g.ptr[n + 1]; ++k) {
+                    const uint32_t m = g.nbr[k];
+                    if (m == n || (m < n) != lower) continue;
+                    ++cnt;
+                    if (m < b || m >= e) continue;  // another slab: through global memory
+                    uint32_t& sl = slot[(size_t)(m - b) * cluster + r];
+                    if (sl == ~0u) {
+                        sl = nslot[c]++;
+                        if (sl >= max_slots) return false;
+                        push[(size_t)m * kPushMax + npush[m]++] = r << 20 | sl;
+                    }
+                    plan.src[k] = sl;
+                }
+                if (cnt > 16) return false;
+            }
+        }
+        max_slot = *std::max_element(nslot.begin(), nslot.end());
+        return true;
+    };
     for (const auto& cs : cand) {
         const uint32_t R = cs.second;
         for (uint32_t n = 0; n < nn; ++n) cta[n] = push_cta(n, nn, n_clusters, cluster, R);
         plan.src.assign(g.nbr.size(), ~0u);
-        if (!push_slots(g, cta, sb, cluster, true, max_slots, plan) ||
-            !push_slots(g, cta, sb, cluster, false, max_slots, plan))
+        if (!slots(true, plan.push_f, plan.nslot_f, plan.max_slot_f) ||
+            !slots(false, plan.push_b, plan.nslot_b, plan.max_slot_b))
             continue;
         plan.n_ctas = nc;
         plan.cluster = cluster;
@@ -291,120 +279,10 @@ bool push_plan(const NodeGraph& g, const std::vector<uint32_t>& fwd_ptr,
         };
         split(fwd_order, lf, plan.pos_f, plan.order_f);
         split(bwd_order, lb, plan.pos_b, plan.order_b);
-        plan.cta = cta;
         return true;
     }
     plan = PushPlan();
     return false;
-}
-
-bool push_plan_chains(const NodeGraph& g, const std::vector<uint32_t>& fwd_ptr,
-                      const std::vector<uint32_t>& fwd_order,
-                      const std::vector<uint32_t>& bwd_ptr,
-                      const std::vector<uint32_t>& bwd_order, uint32_t n_clusters,
-                      uint32_t cluster, uint32_t warps, uint32_t max_slots, PushPlan& plan) {
-    const uint32_t nn = g.n_nodes;
-    plan = PushPlan();
-    if (!nn || !n_clusters || !cluster || cluster > kPushMax || !warps ||
-        fwd_order.size() != nn || bwd_order.size() != nn || fwd_ptr.size() < 2 ||
-        bwd_ptr.size() < 2)
-        return false;
-    const uint32_t nc = n_clusters * cluster, H = 2 * warps;
-    max_slots = std::min(max_slots, 1u << 20);
-    std::vector<uint32_t> lf(nn), lb(nn);
-    for (uint32_t l = 0; l + 1 < fwd_ptr.size(); ++l)
-        for (uint32_t t = fwd_ptr[l]; t < fwd_ptr[l + 1]; ++t) lf[fwd_order[t]] = l;
-    for (uint32_t l = 0; l + 1 < bwd_ptr.size(); ++l)
-        for (uint32_t t = bwd_ptr[l]; t < bwd_ptr[l + 1]; ++t) lb[bwd_order[t]] = l;
-    // chain starts: n = 0 and every n that does not neighbour n - 1
-    std::vector<uint32_t> start;
-    for (uint32_t n = 0; n < nn; ++n) {
-        const uint32_t* b = g.nbr.data() + g.ptr[n];
-        const uint32_t* e = g.nbr.data() + g.ptr[n + 1];
-        if (n == 0 || !std::binary_search(b, e, n - 1)) start.push_back(n);
-    }
-    const uint32_t nch = (uint32_t)start.size();
-    start.push_back(nn);
-    // slabs end at the first chain start at or after s * nn / n_clusters
-    std::vector<uint32_t> sb(n_clusters + 1), chain_of_slab(n_clusters + 1);
-    {
-        uint32_t c = 0;
-        for (uint32_t s = 0; s <= n_clusters; ++s) {
-            const uint64_t t = (uint64_t)s * nn / n_clusters;
-            while (c < nch && start[c] < t) ++c;
-            chain_of_slab[s] = s == n_clusters ? nch : c;
-            sb[s] = start[chain_of_slab[s]];
-        }
-    }
-    // chains round-robin to the CTAs of their slab
-    std::vector<uint32_t> cta(nn);
-    std::vector<std::vector<uint32_t>> chains_of(nc);
-    for (uint32_t s = 0; s < n_clusters; ++s)
-        for (uint32_t c = chain_of_slab[s]; c < chain_of_slab[s + 1]; ++c) {
-            const uint32_t g_ = s * cluster + (c - chain_of_slab[s]) % cluster;
-            chains_of[g_].push_back(c);
-            for (uint32_t n = start[c]; n < start[c + 1]; ++n) cta[n] = g_;
-        }
-    plan.src.assign(g.nbr.size(), ~0u);
-    if (!push_slots(g, cta, sb, cluster, true, max_slots, plan) ||
-        !push_slots(g, cta, sb, cluster, false, max_slots, plan)) {
-        plan = PushPlan();
-        return false;
-    }
-    plan.n_ctas = nc;
-    plan.cluster = cluster;
-    plan.block = 0;
-    plan.warps = warps;
-    plan.cta = cta;
-    auto lay = [&](bool lower, std::vector<uint32_t>& pos, std::vector<uint32_t>& out) {
-        const std::vector<uint32_t>& lev = lower ? lf : lb;
-        pos.assign(nc + 1, 0);
-        out.clear();
-        for (uint32_t c = 0; c < nc; ++c) {
-            // the CTA's chains by the level of their first node in this direction
-            std::vector<std::pair<uint32_t, uint32_t>> ch;  // (level, chain)
-            for (uint32_t k : chains_of[c])
-                ch.push_back({lower ? lev[start[k]] : lev[start[k + 1] - 1], k});
-            std::sort(ch.begin(), ch.end());
-            // nodes of each half in level order (ties by id, in the solve's direction)
-            std::vector<std::vector<uint32_t>> half(H);
-            for (size_t i = 0; i < ch.size(); ++i) {
-                const uint32_t k = ch[i].second;
-                std::vector<uint32_t>& h = half[i % H];
-                for (uint32_t t = 0; t < start[k + 1] - start[k]; ++t)
-                    h.push_back(lower ? start[k] + t : start[k + 1] - 1 - t);
-            }
-            for (std::vector<uint32_t>& h : half)
-                std::stable_sort(h.begin(), h.end(), [&](uint32_t a, uint32_t b) {
-                    return lev[a] < lev[b];
-                });
-            // each warp's steps: its two halves merged by level
-            std::vector<std::vector<std::pair<uint32_t, uint32_t>>> steps(warps);
-            size_t smax = 0;
-            for (uint32_t w = 0; w < warps; ++w) {
-                const std::vector<uint32_t>&A = half[2 * w], &B = half[2 * w + 1];
-                size_t i = 0, j = 0;
-                while (i < A.size() || j < B.size()) {
-                    const uint32_t la = i < A.size() ? lev[A[i]] : ~0u;
-                    const uint32_t lb_ = j < B.size() ? lev[B[j]] : ~0u;
-                    const uint32_t l = std::min(la, lb_);
-                    steps[w].push_back({la == l ? A[i++] : ~0u, lb_ == l ? B[j++] : ~0u});
-                }
-                smax = std::max(smax, steps[w].size());
-            }
-            const size_t base = out.size();
-            out.resize(base + smax * H, ~0u);
-            for (uint32_t w = 0; w < warps; ++w)
-                for (size_t q = 0; q < steps[w].size(); ++q) {
-                    out[base + 2 * w + q * H] = steps[w][q].first;
-                    out[base + 2 * w + 1 + q * H] = steps[w][q].second;
-                }
-            pos[c + 1] = (uint32_t)out.size();
-        }
-    };
-    lay(true, plan.pos_f, plan.order_f);
-    lay(false, plan.pos_b, plan.order_b);
-    return true;
 }
 
 void ilu_edge_maps(const NodeGraph& g, std::vector<uint32_t>& ptr, std::vector<uint8_t>& map) {

@@ -103,10 +103,6 @@ struct PushPlan {
     std::vector<uint32_t> push_f, push_b;
     std::vector<uint32_t> nslot_f, nslot_b;  // slots per CTA
     uint32_t max_slot_f = 0, max_slot_b = 0;
-    std::vector<uint32_t> cta;  // per node: its CTA
-    // 0: positions interleave over any number of warps; else the warps per
-    // CTA the positions were laid out for (push_plan_chains)
-    uint32_t warps = 0;
 };
 
 // CTA of node n: its slab's first CTA plus the round-robin rank of its block
@@ -131,24 +127,5 @@ bool push_plan(const NodeGraph& g, const std::vector<uint32_t>& fwd_ptr,
                const std::vector<uint32_t>& fwd_order, const std::vector<uint32_t>& bwd_ptr,
                const std::vector<uint32_t>& bwd_order, uint32_t n_clusters, uint32_t cluster,
                uint32_t block, uint32_t max_slots, PushPlan& plan);
-
-// The same plan with chains kept together.  A chain is a maximal run of
-// consecutive node ids n0, n0+1, ... in which every node neighbours the one
-// before, so each depends on its predecessor in both solves (the unit
-// cube's x-lines).  Slabs end between chains, a slab's chains are dealt
-// round-robin to its CTAs, and inside a CTA each chain goes to one
-// half-warp (chains sorted by the level of their first node, dealt
-// round-robin over the 2 * warps halves): a half then resolves a chain's
-// nodes one after the other and takes each predecessor's values from its
-// own registers.  Positions are laid out for `warps` warps per CTA: half v
-// = 2w + h takes positions v, v + H, ... (H = 2 * warps) of its CTA, its
-// nodes in level order; the two halves of a warp are merged by level, a
-// hole where only one of them has a node at that level, and every warp is
-// padded with holes to the CTA's longest.  Returns false as push_plan does.
-bool push_plan_chains(const NodeGraph& g, const std::vector<uint32_t>& fwd_ptr,
-                      const std::vector<uint32_t>& fwd_order,
-                      const std::vector<uint32_t>& bwd_ptr,
-                      const std::vector<uint32_t>& bwd_order, uint32_t n_clusters,
-                      uint32_t cluster, uint32_t warps, uint32_t max_slots, PushPlan& plan);
 
 }  // namespace fm

@@ -170,23 +170,14 @@ __device__ __forceinline__ void wait_push(uint32_t sl, const T* gp, unsigned* st
 // runs only over the lanes that can hold neighbours (8 or 16, the same for
 // the whole warp); the other lanes hold zeros, so the sums are those of a
 // full butterfly.  Lanes hl < kPushMax of each half hold its results.
-// pn, p0..p2: the last node this half resolved and its values (a chain's
-// predecessor is taken from them instead of being waited for)
 template <typename T, bool Lower>
 __device__ __forceinline__ void push_node(const PushPre<T>& Q, uint32_t base, T* out,
-                                          unsigned* status, int hl, uint32_t& pn, T& p0, T& p1,
-                                          T& p2) {
+                                          unsigned* status, int hl) {
     const bool has = hl < Q.cnt;
-    const bool own = has && Q.nb == pn;
-    const bool local = has && !own && Q.sv != ~0u;
+    const bool local = has && Q.sv != ~0u;
     T v0, v1, v2;
     wait_push<T>(local ? base + Q.sv * kSlotBytes<T> : ~0u,
-                 has && !own && !local ? out + 3 * (size_t)Q.nb : nullptr, status, v0, v1, v2);
-    if (own) {
-        v0 = p0;
-        v1 = p1;
-        v2 = p2;
-    }
+                 has && !local ? out + 3 * (size_t)Q.nb : nullptr, status, v0, v1, v2);
     T s0 = T(0), s1 = T(0), s2 = T(0);
     if (has) {
         s0 = Q.a[0] * v0 + Q.a[1] * v1 + Q.a[2] * v2;
@@ -215,10 +206,6 @@ __device__ __forceinline__ void push_node(const PushPre<T>& Q, uint32_t base, T*
         x1 = (Q.c[1] - s1 - Q.c[5] * x2) * Q.s[1];
         x0 = (Q.c[0] - s0 - Q.c[3] * x1 - Q.c[4] * x2) * Q.s[0];
     }
-    pn = Q.n;
-    p0 = x0;
-    p1 = x1;
-    p2 = x2;
     if (Q.pe != ~0u)
         st_slot_cluster(mapa(base + (Q.pe & 0xfffffu) * kSlotBytes<T>, Q.pe >> 20), x0, x1, x2);
     if (hl == 0) {
@@ -277,8 +264,6 @@ __global__ void __launch_bounds__(push_max_warps(sizeof(T)) * 32, 1)
         };
         PushPre<T> qa, qb;
         push_pre<T, Lower>(P, S, 0 < mine, rec_of(0, 0), lu, dinv, rhs, hl, qa);
-        uint32_t pn = ~0u;
-        T p0 = T(0), p1 = T(0), p2 = T(0);
         uint32_t q = 0;
         // cur is processed while nxt's loads are in flight; the two swap
         // roles every step (no register copies that would wait on them)
@@ -287,7 +272,7 @@ __global__ void __launch_bounds__(push_max_warps(sizeof(T)) * 32, 1)
             const bool more = q + 1 < nq;
             if (more)
                 push_pre<T, Lower>(P, S, q + 1 < mine, rec_of(q + 1, cb), lu, dinv, rhs, hl, nxt);
-            push_node<T, Lower>(cur, base, out, status, hl, pn, p0, p1, p2);
+            push_node<T, Lower>(cur, base, out, status, hl);
             ++q;
             if ((q & 15) == 0 && more) {
                 ba = bb;

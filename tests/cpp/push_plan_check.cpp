@@ -1,21 +1,18 @@
 // Invariants of the slab-partitioned push solve plan (fm_setup.cpp
 // push_plan), checked on the host for a mesh given as argv:
-//   push_plan_check N seed clusters cluster [block [max_slots [chain_warps]]]
-// (chain_warps > 0: the chain-keeping plan, push_plan_chains, laid out for
-// that many warps per CTA)
+//   push_plan_check N seed clusters cluster [block [max_slots]]
 // builds the N^3 unit cube (seed > 0: node ids randomly relabelled; seed
 // < 0: relabelled inside blocks of 8 consecutive ids) and checks, for both
 // directions:
 //   * a refused plan only where some node has more than 16 neighbours on
 //     one side;
 //   * the position ranges of the CTAs tile the orders; each CTA's range lists
-//     exactly the nodes the plan assigns it plus holes; slabs are contiguous
-//     node ranges; the range has even length and positions 2i, 2i + 1
-//     (resolved together by one warp) are never two nodes of different
-//     levels; the interleaved plan: the range is in non-decreasing
-//     dependency level and no CTA holds more than max_level_share nodes of
-//     one level; the chain plan: every warp's positions are in
-//     non-decreasing level, and a chain's nodes all sit in one half-warp;
+//     exactly the nodes push_cta assigns it plus holes, with non-decreasing
+//     dependency level (so every warp meets a node only after all nodes it
+//     waits on are reachable); the range has even length and positions 2i,
+//     2i + 1 (resolved together by one warp) are never two nodes of
+//     different levels; no CTA holds more than max_level_share nodes of one
+//     level;
 //   * every neighbour entry on the solve's side reads from a slot exactly
 //     when the neighbour is in the reader's slab; that slot lies inside the
 //     reader CTA's slot count, holds only that neighbour, and the
@@ -51,7 +48,6 @@ int main(int argc, char** argv) {
     const uint32_t cs = argc > 4 ? (uint32_t)std::atoi(argv[4]) : 8;
     const uint32_t block = argc > 5 ? (uint32_t)std::atoi(argv[5]) : 0;
     const uint32_t max_slots = argc > 6 ? (uint32_t)std::atoi(argv[6]) : (1u << 20);
-    const uint32_t chain_warps = argc > 7 ? (uint32_t)std::atoi(argv[7]) : 0;
     const uint32_t nn = (N + 1) * (N + 1) * (N + 1), ne = 6 * N * N * N;
     std::vector<double> xyz(3 * (size_t)nn);
     std::vector<uint32_t> conn(4 * (size_t)ne);
@@ -72,10 +68,7 @@ int main(int argc, char** argv) {
     node_levels(g, true, fp, fo);
     node_levels(g, false, bp, bo);
     PushPlan P;
-    const bool ok = chain_warps
-                        ? push_plan_chains(g, fp, fo, bp, bo, ncl, cs, chain_warps, max_slots, P)
-                        : push_plan(g, fp, fo, bp, bo, ncl, cs, block, max_slots, P);
-    if (!ok) {
+    if (!push_plan(g, fp, fo, bp, bo, ncl, cs, block, max_slots, P)) {
         uint32_t side = 0;
         for (uint32_t n = 0; n < nn; ++n) {
             uint32_t lo = 0, hi = 0;
@@ -85,7 +78,7 @@ int main(int argc, char** argv) {
             }
             side = std::max(side, std::max(lo, hi));
         }
-        if (side > 16 || (chain_warps && max_slots < (1u << 20))) {
+        if (side > 16) {
             std::printf("ok\n");  // refused as documented
             return 0;
         }
@@ -93,24 +86,15 @@ int main(int argc, char** argv) {
     }
     const uint32_t nc = ncl * cs;
     if (P.n_ctas != nc || P.cluster != cs || P.pos_f.size() != nc + 1 ||
-        P.pos_b.size() != nc + 1 || P.cta.size() != nn)
+        P.pos_b.size() != nc + 1 || !P.block || (block && P.block != block))
         return fail("plan shape", P.n_ctas, P.block);
-    if (chain_warps ? (P.warps != chain_warps || P.block)
-                    : (P.warps || !P.block || (block && P.block != block)))
-        return fail("plan kind", P.warps, P.block);
-    const std::vector<uint32_t>& cta = P.cta;
+    std::vector<uint32_t> cta(nn);
     for (uint32_t n = 0; n < nn; ++n) {
+        cta[n] = push_cta(n, nn, ncl, cs, P.block);
         if (cta[n] >= nc) return fail("CTA out of range", n, cta[n]);
-        if (!chain_warps && cta[n] != push_cta(n, nn, ncl, cs, P.block))
-            return fail("CTA not the interleaved one", n, cta[n]);
-        if (n && cta[n] / cs < cta[n - 1] / cs) return fail("slabs not contiguous", n, cta[n]);
-    }
-    // chains: node n continues n - 1's chain when it neighbours it
-    std::vector<uint32_t> chain(nn, 0);
-    for (uint32_t n = 1; n < nn; ++n) {
-        const uint32_t* b = g.nbr.data() + g.ptr[n];
-        const uint32_t* e = g.nbr.data() + g.ptr[n + 1];
-        chain[n] = std::binary_search(b, e, n - 1) ? chain[n - 1] : n;
+        const uint32_t sl = cta[n] / cs;
+        if (n < push_slab_begin(sl, nn, ncl) || n >= push_slab_begin(sl + 1, nn, ncl))
+            return fail("node outside its slab", n, sl);
     }
     for (int lower = 1; lower >= 0; --lower) {
         const std::vector<uint32_t>& lp = lower ? fp : bp;
@@ -134,10 +118,6 @@ int main(int argc, char** argv) {
                 return fail("position range decreasing or odd", c, 0);
             uint32_t run = 0;
             long prev = -1;  // last node of the range so far
-            const uint32_t H = 2 * chain_warps;
-            std::vector<long> wlast(chain_warps, -1);   // last level met by each warp
-            std::vector<long> hchain(H, -1);            // chains met by each half
-            std::vector<long> chain_half(0);
             for (uint32_t t = pos[c]; t < pos[c + 1]; ++t) {
                 const uint32_t n = ord[t];
                 if (((t - pos[c]) & 1) && n != ~0u && ord[t - 1] != ~0u &&
@@ -146,19 +126,11 @@ int main(int argc, char** argv) {
                 if (n == ~0u) continue;
                 if (n >= nn || cta[n] != c) return fail("node in foreign CTA", c, t);
                 if (seen[n]++) return fail("node listed twice", c, n);
-                if (chain_warps) {
-                    const uint32_t v = (t - pos[c]) % H, w = v / 2;
-                    if (wlast[w] > (long)level[n]) return fail("warp order not by level", c, t);
-                    wlast[w] = level[n];
-                    continue;
-                }
                 if (prev >= 0 && level[n] < level[prev]) return fail("CTA order not by level", c, t);
                 run = prev >= 0 && level[n] == level[prev] ? run + 1 : 1;
                 if (run > P.max_level_share) return fail("level share above max", c, t);
                 prev = n;
             }
-            (void)hchain;
-            (void)chain_half;
         }
         // (reader CTA, slot) -> producer; push entries actually read
         std::vector<std::vector<long>> owner(nc);
@@ -195,21 +167,8 @@ int main(int argc, char** argv) {
                 if (!found) return fail("producer does not push to its reader", m, n);
             }
         }
-        // chain plan: a chain's nodes all sit in one half-warp of one CTA
-        if (chain_warps) {
-            const uint32_t H = 2 * chain_warps;
-            std::vector<long> half_of(nn, -1);
-            for (uint32_t c = 0; c < nc; ++c)
-                for (uint32_t t = pos[c]; t < pos[c + 1]; ++t)
-                    if (ord[t] != ~0u) half_of[ord[t]] = (long)c * H + (t - pos[c]) % H;
-            for (uint32_t n = 1; n < nn; ++n)
-                if (chain[n] == chain[n - 1] && half_of[n] != half_of[n - 1])
-                    return fail("chain split over half-warps", n, half_of[n]);
-        }
         // schedule simulation: every warp advances while its next pair is ready
-        std::vector<uint32_t> Ws = {1u, 3u, 16u, 24u};
-        if (chain_warps) Ws = {chain_warps};
-        for (uint32_t W : Ws) {
+        for (uint32_t W : {1u, 3u, 16u, 24u}) {
             const uint32_t H = 2 * W;
             std::vector<uint8_t> done(nn, 0);
             std::vector<uint32_t> q((size_t)nc * W, 0);
@@ -260,9 +219,6 @@ int main(int argc, char** argv) {
             }
         }
     }
-    if (getenv("PUSH_PLAN_STATS"))
-        std::printf("positions %zu / %zu nodes forward, %zu backward, slots %u / %u\n",
-                    P.order_f.size(), (size_t)nn, P.order_b.size(), P.max_slot_f, P.max_slot_b);
     std::printf("ok\n");
     return 0;
 }

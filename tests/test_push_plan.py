@@ -32,8 +32,7 @@ def push_exe(tmp_path_factory):
     (6, 7, 16, 8, 0, 1 << 20), (12, -11, 3, 8, 0, 1 << 20), (1, 0, 16, 8, 0, 1 << 20),
     (2, 5, 4, 2, 0, 1 << 20), (12, 0, 16, 8, 65, 1 << 20), (12, 0, 4, 8, 0, 300),
     (10, -3, 15, 8, 0, 1 << 20)])
-@pytest.mark.parametrize("chain_warps", [0, 16, 3])
-def test_push_plan_invariants(push_exe, N, seed, ncl, cs, block, limit, chain_warps):
-    r = subprocess.run([push_exe, str(N), str(seed), str(ncl), str(cs), str(block), str(limit),
-                        str(chain_warps)], capture_output=True, text=True, timeout=300)
+def test_push_plan_invariants(push_exe, N, seed, ncl, cs, block, limit):
+    r = subprocess.run([push_exe, str(N), str(seed), str(ncl), str(cs), str(block), str(limit)],
+                       capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
