@@ -400,7 +400,9 @@ fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
     const char* path = getenv("FM_TRSV_PATH");
     if (path && std::strcmp(path, "push") != 0) return FM_OK;
     constexpr uint32_t kCluster = 8;
-    constexpr size_t kMaxSmem = 227 * 1024;
+    // dynamic shared memory per CTA at most; the kernels' static shared
+    // memory (under 1 KB) takes the rest of the 227 KB
+    constexpr size_t kMaxSmem = 226 * 1024;
     auto env = [](const char* name, int dflt, int lo_, int hi) {
         const char* v = getenv(name);
         return v ? std::min(hi, std::max(lo_, atoi(v))) : dflt;
@@ -450,6 +452,9 @@ fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
     v.push_b = c->pu_push_b.p;
     v.nslot_f = c->pu_nslot_f.p;
     v.nslot_b = c->pu_nslot_b.p;
+    // FM_TRSV_PUSH_INDEP=1: half-warps resolve their nodes independently
+    v.indep = getenv("FM_TRSV_PUSH_INDEP") && atoi(getenv("FM_TRSV_PUSH_INDEP")) ? 1u : 0u;
+
     c->pu = v;
     c->pu_ok32 = ok32;
     c->pu_ok64 = ok64;

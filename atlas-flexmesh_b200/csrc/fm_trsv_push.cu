@@ -131,8 +131,8 @@ __device__ __forceinline__ void push_pre(const PushSolve& P, const NodeSched& S,
 // neighbour).  On a timeout FM_FLAG_TIMEOUT is set and the values may
 // still be sentinels.
 template <typename T>
-__device__ __forceinline__ void wait_push(uint32_t sl, const T* gp, unsigned* status, T& v0,
-                                          T& v1, T& v2) {
+__device__ __forceinline__ void wait_push(uint32_t sl, const T* gp, unsigned* status,
+                                          unsigned m, T& v0, T& v1, T& v2) {
     v0 = v1 = v2 = T(0);
     auto poll = [&]() {
         if (sl != ~0u) {
@@ -149,17 +149,17 @@ __device__ __forceinline__ void wait_push(uint32_t sl, const T* gp, unsigned* st
         v0 = v1 = v2 = Sentinel<T>::value();
         need = poll();
     }
-    if (!__any_sync(kFull, need)) return;
+    if (!__any_sync(m, need)) return;
     const long long t0 = clock64(), limit = wait_limit(status);
     for (unsigned it = 1;; ++it) {
         if (need) need = poll();
-        if (!__any_sync(kFull, need)) return;
+        if (!__any_sync(m, need)) return;
         // shared-memory polls are short: look at the clock and the grid's
         // timeout flag every 256 rounds
         if ((it & 255u) == 0 &&
-            __any_sync(kFull, (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) ||
-                                  clock64() - t0 > limit)) {
-            if ((threadIdx.x & 31) == 0) raise_flag(status, FM_FLAG_TIMEOUT);
+            __any_sync(m, (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) ||
+                              clock64() - t0 > limit)) {
+            if ((threadIdx.x & 15) == 0) raise_flag(status, FM_FLAG_TIMEOUT);
             return;
         }
     }
@@ -172,28 +172,28 @@ __device__ __forceinline__ void wait_push(uint32_t sl, const T* gp, unsigned* st
 // full butterfly.  Lanes hl < kPushMax of each half hold its results.
 template <typename T, bool Lower>
 __device__ __forceinline__ void push_node(const PushPre<T>& Q, uint32_t base, T* out,
-                                          unsigned* status, int hl) {
+                                          unsigned* status, int hl, unsigned m) {
     const bool has = hl < Q.cnt;
     const bool local = has && Q.sv != ~0u;
     T v0, v1, v2;
     wait_push<T>(local ? base + Q.sv * kSlotBytes<T> : ~0u,
-                 has && !local ? out + 3 * (size_t)Q.nb : nullptr, status, v0, v1, v2);
+                 has && !local ? out + 3 * (size_t)Q.nb : nullptr, status, m, v0, v1, v2);
     T s0 = T(0), s1 = T(0), s2 = T(0);
     if (has) {
         s0 = Q.a[0] * v0 + Q.a[1] * v1 + Q.a[2] * v2;
         s1 = Q.a[3] * v0 + Q.a[4] * v1 + Q.a[5] * v2;
         s2 = Q.a[6] * v0 + Q.a[7] * v1 + Q.a[8] * v2;
     }
-    if (__any_sync(kFull, Q.cnt > 8)) {
-        s0 += __shfl_xor_sync(kFull, s0, 8);
-        s1 += __shfl_xor_sync(kFull, s1, 8);
-        s2 += __shfl_xor_sync(kFull, s2, 8);
+    if (__any_sync(m, Q.cnt > 8)) {
+        s0 += __shfl_xor_sync(m, s0, 8);
+        s1 += __shfl_xor_sync(m, s1, 8);
+        s2 += __shfl_xor_sync(m, s2, 8);
     }
 #pragma unroll
     for (int o = 4; o; o >>= 1) {
-        s0 += __shfl_xor_sync(kFull, s0, o);
-        s1 += __shfl_xor_sync(kFull, s1, o);
-        s2 += __shfl_xor_sync(kFull, s2, o);
+        s0 += __shfl_xor_sync(m, s0, o);
+        s1 += __shfl_xor_sync(m, s1, o);
+        s2 += __shfl_xor_sync(m, s2, o);
     }
     if (Q.n == ~0u) return;
     T x0, x1, x2;
@@ -216,9 +216,9 @@ __device__ __forceinline__ void push_node(const PushPre<T>& Q, uint32_t base, T*
     }
 }
 
-__device__ __forceinline__ uint4 shfl4(uint4 v, int src) {
-    return make_uint4(__shfl_sync(kFull, v.x, src), __shfl_sync(kFull, v.y, src),
-                      __shfl_sync(kFull, v.z, src), __shfl_sync(kFull, v.w, src));
+__device__ __forceinline__ uint4 shfl4(uint4 v, int src, unsigned m) {
+    return make_uint4(__shfl_sync(m, v.x, src), __shfl_sync(m, v.y, src),
+                      __shfl_sync(m, v.z, src), __shfl_sync(m, v.w, src));
 }
 
 // One direction.  fill/n_fill: a vector the kernel sets to the wait
@@ -246,10 +246,13 @@ __global__ void __launch_bounds__(push_max_warps(sizeof(T)) * 32, 1)
     const uint32_t beg = pos[g], end = pos[g + 1];
     const uint32_t v0 = 2 * (threadIdx.x >> 5), v = v0 + (uint32_t)(lane >> 4);
     const uint4* rec = Lower ? P.rec_f : P.rec_b;
-    if (beg + v0 < end) {
-        // steps of the warp: the first half's count (it starts first)
-        const uint32_t nq = (end - beg - v0 + H - 1) / H;
-        const uint32_t mine = beg + v < end ? (end - beg - v + H - 1) / H : 0;
+    // P.indep: the two halves run independently (votes and shuffles over
+    // the half), else in lock step over the warp
+    const unsigned m = P.indep ? ((lane & 16) ? 0xffff0000u : 0x0000ffffu) : kFull;
+    const uint32_t mine = beg + v < end ? (end - beg - v + H - 1) / H : 0;
+    if (P.indep ? mine > 0 : beg + v0 < end) {
+        // steps: the half's own count, or the warp's (the first half's: it starts first)
+        const uint32_t nq = P.indep ? mine : (end - beg - v0 + H - 1) / H;
         // records come 16 per half-warp, one per lane, a batch ahead of use,
         // and are handed out by shuffles: no record load is ever waited on
         const uint4 zero = make_uint4(0, 0, 0, 0);
@@ -260,7 +263,7 @@ __global__ void __launch_bounds__(push_max_warps(sizeof(T)) * 32, 1)
         uint4 ba = batch(0), bb = batch(1);
         // record q of this half's batch cb or cb + 1
         auto rec_of = [&](uint32_t q, uint32_t cb) {
-            return shfl4((q >> 4) == cb ? ba : bb, (lane & 16) | (int)(q & 15));
+            return shfl4((q >> 4) == cb ? ba : bb, (lane & 16) | (int)(q & 15), m);
         };
         PushPre<T> qa, qb;
         push_pre<T, Lower>(P, S, 0 < mine, rec_of(0, 0), lu, dinv, rhs, hl, qa);
@@ -272,7 +275,7 @@ __global__ void __launch_bounds__(push_max_warps(sizeof(T)) * 32, 1)
             const bool more = q + 1 < nq;
             if (more)
                 push_pre<T, Lower>(P, S, q + 1 < mine, rec_of(q + 1, cb), lu, dinv, rhs, hl, nxt);
-            push_node<T, Lower>(cur, base, out, status, hl);
+            push_node<T, Lower>(cur, base, out, status, hl, m);
             ++q;
             if ((q & 15) == 0 && more) {
                 ba = bb;
@@ -291,6 +294,7 @@ __global__ void __launch_bounds__(push_max_warps(sizeof(T)) * 32, 1)
              i += gridDim.x * blockDim.x)
             fill[i] = sv;
     }
+    __syncwarp();  // independent halves reconverge before the aligned barrier
     cluster_barrier();  // no CTA leaves while a store into its slots may be in flight
 }
 
