@@ -452,8 +452,6 @@ fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
     v.push_b = c->pu_push_b.p;
     v.nslot_f = c->pu_nslot_f.p;
     v.nslot_b = c->pu_nslot_b.p;
-    // FM_TRSV_PUSH_INDEP=1: half-warps resolve their nodes independently
-    v.indep = getenv("FM_TRSV_PUSH_INDEP") && atoi(getenv("FM_TRSV_PUSH_INDEP")) ? 1u : 0u;
 
     c->pu = v;
     c->pu_ok32 = ok32;

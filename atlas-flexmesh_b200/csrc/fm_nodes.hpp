@@ -55,9 +55,6 @@ struct PushSolve {
     const uint32_t* push_b = nullptr;
     const uint32_t* nslot_f = nullptr;  // slots per CTA
     const uint32_t* nslot_b = nullptr;
-    // 1: the two half-warps of a warp resolve their nodes independently
-    // (each waits and reduces over its own 16 lanes); 0: in lock step
-    uint32_t indep = 0;
 };
 // most warps per CTA of the push kernels of this value width (register budget)
 constexpr int push_max_warps(size_t value_bytes) { return value_bytes == 4 ? 24 : 16; }

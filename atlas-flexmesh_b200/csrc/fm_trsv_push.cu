@@ -246,13 +246,11 @@ __global__ void __launch_bounds__(push_max_warps(sizeof(T)) * 32, 1)
     const uint32_t beg = pos[g], end = pos[g + 1];
     const uint32_t v0 = 2 * (threadIdx.x >> 5), v = v0 + (uint32_t)(lane >> 4);
     const uint4* rec = Lower ? P.rec_f : P.rec_b;
-    // P.indep: the two halves run independently (votes and shuffles over
-    // the half), else in lock step over the warp
-    const unsigned m = P.indep ? ((lane & 16) ? 0xffff0000u : 0x0000ffffu) : kFull;
-    const uint32_t mine = beg + v < end ? (end - beg - v + H - 1) / H : 0;
-    if (P.indep ? mine > 0 : beg + v0 < end) {
-        // steps: the half's own count, or the warp's (the first half's: it starts first)
-        const uint32_t nq = P.indep ? mine : (end - beg - v0 + H - 1) / H;
+    const unsigned m = kFull;  // both halves vote and shuffle over the whole warp
+    if (beg + v0 < end) {
+        // steps of the warp: the first half's count (it starts first)
+        const uint32_t nq = (end - beg - v0 + H - 1) / H;
+        const uint32_t mine = beg + v < end ? (end - beg - v + H - 1) / H : 0;
         // records come 16 per half-warp, one per lane, a batch ahead of use,
         // and are handed out by shuffles: no record load is ever waited on
         const uint4 zero = make_uint4(0, 0, 0, 0);
@@ -294,7 +292,6 @@ __global__ void __launch_bounds__(push_max_warps(sizeof(T)) * 32, 1)
              i += gridDim.x * blockDim.x)
             fill[i] = sv;
     }
-    __syncwarp();  // independent halves reconverge before the aligned barrier
     cluster_barrier();  // no CTA leaves while a store into its slots may be in flight
 }
 
