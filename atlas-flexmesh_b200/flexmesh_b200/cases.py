@@ -142,7 +142,7 @@ def case_ilu(a):
     return {"case": "ilu", "N": a.N, "prec": a.prec, "reps": prof["calls"],
             "ms_per_factorization": round(per, 3), "bytes": B,
             "achieved_gbs": round(B / per / 1e6, 1), "peak_gbs": peak, "peak_kind": kind,
-            "frac": round(B / per / 1e6 / peak, 4)}
+            "frac": round(B / per / 1e6 / peak, 4), "flags": ctx.flags()}
 
 
 def case_assemble(a):
