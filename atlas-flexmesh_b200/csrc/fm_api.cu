@@ -77,7 +77,6 @@ struct fm_ctx {
     // node-block schedule of the solve pattern (ILU(0) and triangular solves)
     DevBuf<uint32_t> self_pos, node_fwd, node_bwd, emap_ptr;
     DevBuf<uint8_t> emap;  // ILU(0) update map
-    DevBuf<uint8_t> ilu_split;  // per node: its lower neighbours before the first one a level below
     DevBuf<uint4> node_fwd_rec, node_bwd_rec;
     uint32_t node_levels_fwd = 0, node_levels_bwd = 0, width_fwd = 0, width_bwd = 0;
     std::vector<uint32_t> lvl_fwd_ptr, lvl_fwd_rows, lvl_bwd_ptr, lvl_bwd_rows;
@@ -371,7 +370,6 @@ fm::NodeSched node_sched(const fm_ctx* c) {
     S.max_width_bwd = c->width_bwd;
     S.emap_ptr = c->emap_ptr.p;
     S.emap = c->emap.p;
-    S.ilu_split = c->ilu_split.p;
     return S;
 }
 
@@ -860,23 +858,6 @@ fm_status fm_set_mesh(fm_ctx* c, uint32_t n_nodes, const double* xyz, uint32_t n
         for (size_t l = 0; l + 1 < c->node_up.size(); ++l)
             c->width_bwd = std::max(c->width_bwd, c->node_up[l + 1] - c->node_up[l]);
         TRY(setup_push_solves(c, c->node_lp, c->node_lo, c->node_up, c->node_uo));
-        {
-            // ILU(0) split: the lower neighbours (ascending) before the first
-            // one exactly one level below the node, which the factorization
-            // eliminates while the later ones are still being finished
-            std::vector<uint32_t> lev(n_nodes);
-            for (uint32_t l = 0; l + 1 < c->node_lp.size(); ++l)
-                for (uint32_t t = c->node_lp[l]; t < c->node_lp[l + 1]; ++t)
-                    lev[c->node_lo[t]] = l;
-            std::vector<uint8_t> split(n_nodes, 0);
-            const fm::NodeGraph& g = c->graph;
-            for (uint32_t n = 0; n < n_nodes; ++n) {
-                uint32_t k = 0;
-                while (k < g.self[n] && lev[g.nbr[g.ptr[n] + k]] + 1 != lev[n]) ++k;
-                split[n] = (uint8_t)std::min<uint32_t>(k, 255);
-            }
-            CK(upload(c->ilu_split, split.data(), split.size(), c->stream));
-        }
         CK(cudaStreamSynchronize(c->stream));
         CK(c->done.reserve(std::max<size_t>(c->done.n, (size_t)c->nn + 1)));
         CK(cudaMemsetAsync(c->done.p, 0, c->done.n * sizeof(unsigned), c->stream));

@@ -175,12 +175,8 @@ __global__ void __launch_bounds__(kNodeWarps * 32, sizeof(T) == 4 ? 3 : 2)
         const bool fast = sk > 0 && sk <= cap_k && sk <= kStageNbrs &&
                           tot <= (uint32_t)(32 * kPairRound);
         const T* fsrc[kPairRound];
-        int fmrl[kPairRound], fjb[kPairRound], flim[kPairRound], fdst[kPairRound], fk[kPairRound];
+        int fmrl[kPairRound], fjb[kPairRound], flim[kPairRound], fdst[kPairRound];
         uint32_t fpos[kPairRound];
-        // early neighbours (fast path): eliminated as soon as they are final,
-        // while the ones a level below the node, which come later, are still
-        // being finished by other warps
-        const int e = fast && S.ilu_split ? min((int)__ldg(S.ilu_split + n), sk) : 0;
         if (fast) {
             for (int i = lane; i < sk * 3 * rs; i += 32) G.u[i] = T(0);
             __syncwarp();
@@ -190,7 +186,7 @@ __global__ void __launch_bounds__(kNodeWarps * 32, sizeof(T) == 4 ? 3 : 2)
                 fpos[r] = 0xffu;
                 fdst[r] = 0;
                 fsrc[r] = nullptr;
-                fmrl[r] = fjb[r] = flim[r] = fk[r] = 0;
+                fmrl[r] = fjb[r] = flim[r] = 0;
                 if (pr < tot) {
                     int k = 0;
                     for (int kk = 1; kk < sk; ++kk) k += (int)(G.poff[kk] <= pr);
@@ -202,28 +198,24 @@ __global__ void __launch_bounds__(kNodeWarps * 32, sizeof(T) == 4 ? 3 : 2)
                     flim[r] = 3 * ms;
                     fsrc[r] = lu + 9 * (size_t)G.mb0[k] + 3 * kk;
                     fdst[r] = (k * 3) * rs;
-                    fk[r] = k;
                 }
             }
         }
+        // wait for every lower neighbour node's rows
+        const bool ok = wait_flags_warp(done + (lane < sk ? my_nbr : 0), lane < sk, epoch,
+                                        status, sleep_ns);
         T dv0 = T(0), dv1 = T(0), dv2 = T(0);
-        // fast path: wait for lower neighbours k0 <= k < k1, stage their U
-        // rows, eliminate them (the two phases split at e)
-        auto fast_phase = [&](int k0, int k1) {
-            const bool mine = lane >= k0 && lane < k1;
-            const bool okp = wait_flags_warp(done + (mine ? my_nbr : 0), mine, epoch, status,
-                                             sleep_ns);
-            if (okp && mine) {
-                dv0 = ld_cg(dinv + 3 * (size_t)my_nbr);
-                dv1 = ld_cg(dinv + 3 * (size_t)my_nbr + 1);
-                dv2 = ld_cg(dinv + 3 * (size_t)my_nbr + 2);
-            }
-            __syncwarp();
-            if (!okp) return false;
+        if (ok && lane < sk) {
+            dv0 = ld_cg(dinv + 3 * (size_t)my_nbr);
+            dv1 = ld_cg(dinv + 3 * (size_t)my_nbr + 1);
+            dv2 = ld_cg(dinv + 3 * (size_t)my_nbr + 2);
+        }
+        __syncwarp();
+        if (ok && fast) {
             T val[kPairRound][9];
 #pragma unroll
             for (int r = 0; r < kPairRound; ++r)
-                if (fpos[r] != 0xffu && fk[r] >= k0 && fk[r] < k1)
+                if (fpos[r] != 0xffu)
 #pragma unroll
                     for (int q = 0; q < 3; ++q)
 #pragma unroll
@@ -233,7 +225,7 @@ __global__ void __launch_bounds__(kNodeWarps * 32, sizeof(T) == 4 ? 3 : 2)
                                                     : T(0);
 #pragma unroll
             for (int r = 0; r < kPairRound; ++r)
-                if (fpos[r] != 0xffu && fk[r] >= k0 && fk[r] < k1) {
+                if (fpos[r] != 0xffu) {
                     const int d = fdst[r] + 3 * (int)fpos[r];
 #pragma unroll
                     for (int q = 0; q < 3; ++q)
@@ -243,23 +235,7 @@ __global__ void __launch_bounds__(kNodeWarps * 32, sizeof(T) == 4 ? 3 : 2)
             __syncwarp();
 #pragma unroll
             for (int k = 0; k < kStageNbrs; ++k)
-                if (k >= k0 && k < k1) ilu_step(G, w, k, 0, rs, nsl, lane, dv0, dv1, dv2);
-            __syncwarp();
-            return true;
-        };
-        bool ok;
-        if (fast) {
-            ok = e > 0 ? fast_phase(0, e) : true;
-            if (ok) ok = fast_phase(e, sk);
-        } else {
-            // wait for every lower neighbour node's rows
-            ok = wait_flags_warp(done + (lane < sk ? my_nbr : 0), lane < sk, epoch, status,
-                                 sleep_ns);
-            if (ok && lane < sk) {
-                dv0 = ld_cg(dinv + 3 * (size_t)my_nbr);
-                dv1 = ld_cg(dinv + 3 * (size_t)my_nbr + 1);
-                dv2 = ld_cg(dinv + 3 * (size_t)my_nbr + 2);
-            }
+                if (k < sk) ilu_step(G, w, k, 0, rs, nsl, lane, dv0, dv1, dv2);
             __syncwarp();
         }
         for (int k0 = 0; ok && !fast && k0 < sk; k0 += cap_k) {
@@ -404,15 +380,8 @@ void launch_ilu0_nodes(const NodeSched& S, const T* a, T* lu, T* d, T* dinv, uns
         const char* v = getenv("FM_ILU_SLEEP_NS");
         return v ? (unsigned)strtoul(v, nullptr, 10) : 0u;
     }();
-    // FM_ILU_SPLIT=0: wait for every lower neighbour before eliminating any
-    static const bool split = [] {
-        const char* v = getenv("FM_ILU_SPLIT");
-        return !(v && v[0] == '0');
-    }();
-    NodeSched Sl = S;
-    if (!split) Sl.ilu_split = nullptr;
     k_ilu0_nodes<T><<<grid_for(res[f], S.max_width_fwd), kNodeWarps * 32, smem, s>>>(
-        Sl, a, lu, d, dinv, done, epoch, status, sleep_ns);
+        S, a, lu, d, dinv, done, epoch, status, sleep_ns);
 }
 
 template void launch_ilu0_nodes<double>(const NodeSched&, const double*, double*, double*,

@@ -24,9 +24,6 @@ struct NodeSched {
     // ILU(0) update map (fm_setup.cpp ilu_edge_maps): per node offset, entries
     const uint32_t* emap_ptr = nullptr;
     const uint8_t* emap = nullptr;
-    // per node: how many of its lower neighbours (ascending) come before the
-    // first one a single level below it (may be null: none)
-    const uint8_t* ilu_split = nullptr;
 };
 
 // y = U^-1 L^-1 r using tmp for the intermediate (both overwritten);
