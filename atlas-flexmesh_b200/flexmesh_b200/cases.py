@@ -120,6 +120,8 @@ def case_trsv(a):
             "ms_per_apply": round(per, 4), "bytes_per_apply": B,
             "achieved_gbs": round(B / per / 1e6, 1), "peak_gbs": peak, "peak_kind": kind,
             "frac": round(B / per / 1e6 / peak, 4), "wall_ms": round(t.ms, 2),
+            "spmv_ms_per_call": round(prof["spmv"]["ms"] / prof["spmv"]["calls"], 4)
+            if prof.get("spmv", {}).get("calls") else None,
             "flags": ctx.flags()}
 
 

@@ -245,13 +245,18 @@ def run_flexmesh(args, rank, world, local, dist):
         r = ctx.newton_step_cfg(uh, lvl / S, **mixed)
         e_newton += r["newton_iters"]
     te = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([te], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
     e2e_same = bool((torch.from_numpy(uh).to(dev) == up).all().item())
 
-    # the plain FP64 path over the same complete load path
+    # the plain FP64 path over the same complete load path (rank 0: the
+    # replicas would repeat it; no collective inside)
     fp = None
-    if not args.no_fp64:
+    if not args.no_fp64 and rank == 0:
         u64 = torch.zeros_like(u)
-        barrier()
+        torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         n64 = p64 = 0
@@ -262,7 +267,7 @@ def run_flexmesh(args, rank, world, local, dist):
             p64 += r["pcg_iters"]
             lv64.append((lvl, r["newton_iters"], r["pcg_iters"]))
         e1.record(stream)
-        barrier()
+        torch.cuda.synchronize()
         t64 = e0.elapsed_time(e1) / 1e3
         err = (torch.linalg.norm(up - u64) / torch.linalg.norm(u64)).item()
         t_mixed_path = sum(paths) / len(paths) if paths else None
