@@ -312,60 +312,64 @@ def case_adjoint(a):
 
 def case_incompressible(a):
     """Near-incompressible block (48^3 x 6 tets, jitter 0.1 h, nu = 0.49,
-    u_z = -0.4 in 20 load steps): mixed-precision Newton against FP64, PCG
-    iterations per load step, and the adjoint dL/dmu for
-    L = 1/2 |u_top - u*|^2 with u* from a log-normal mu field (sigma 0.2)."""
+    u_z = -0.4 in 20 load steps), the whole load path in mixed precision and
+    in FP64 with the same inexact-Newton settings (inner PCG to a.inner_tol,
+    ILU(0) every a.ilu_every solves, the engine's line search; mixed starts
+    each correction's PCG from the projected previous one), Newton and PCG
+    counts per load step, the mixed-vs-FP64 difference at the end, and the
+    adjoint dL/dmu (FP64 and mixed) for L = 1/2 |u_top - u*|^2 with u* from
+    the log-normal mu field (sigma 0.2).  The reference's tangent clamps its
+    volumetric term at max(1 - 2 nu, 0.1) = 0.1 against the exact 0.02, so
+    Newton contracts by about 0.99 per iteration here: thousands of
+    iterations per load step, each cheap."""
     P = configs.near_incompressible_block(a.N)
     nu = P.nu
     ctx = problem_context(P)
     n = ctx.n_dofs
     out = {"case": "incompressible", "N": a.N, "tets": ctx.n_elems, "nu": nu,
-           "load_steps": P.n_steps}
-    # mixed precision over the whole load path, FP64 over its first
-    # a.fp64_steps load steps (the FP64 solves dominate the run time)
-    k64 = min(a.fp64_steps, P.n_steps)
-    runs = {}
-    for name, prec, inner, steps in (("mixed", L.FM_MIXED, a.inner_tol, P.n_steps),
-                                     ("fp64", L.FM_FP64, 1e-12, k64)):
+           "load_steps": P.n_steps, "inner_tol": a.inner_tol, "ilu_every": a.ilu_every}
+    base = dict(newton_rtol=1e-10, inner_tol=a.inner_tol, predictor_tol=1e-6,
+                max_newton=a.max_newton, max_pcg=20000, line_search=10, ls_c=1e-4,
+                ilu_every=a.ilu_every)
+
+    def path(prec, label):
+        cfg = dict(base, prec=prec, initial_guess=1 if prec == L.FM_MIXED else 0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         u = torch.zeros(n, dtype=torch.float64, device="cuda")
         per = []
-        for s in range(1, steps + 1):
-            r = ctx.newton_step(u, s / P.n_steps, rtol=1e-10, inner_tol=inner,
-                                max_newton=a.max_newton, max_pcg=20000,
-                                line_search=a.line_search, prec=prec)
+        for s in range(1, P.n_steps + 1):
+            r = ctx.newton_step_cfg(u, s / P.n_steps, **cfg)
             per.append((r["newton_iters"], r["pcg_iters"]))
-            print(f"[{name}] step {s}: newton {per[-1][0]} pcg {per[-1][1]} "
+            print(f"[{label}] step {s}: newton {per[-1][0]} pcg {per[-1][1]} "
                   f"t {time.perf_counter() - t0:.1f}s", file=sys.stderr, flush=True)
-            if name == "mixed" and s == k64:
-                runs["mixed_at_fp64_steps"] = u.clone()
         torch.cuda.synchronize()
-        runs[name] = u
-        out[name] = {"s": round(time.perf_counter() - t0, 2), "load_steps": steps,
-                     "newton": sum(k for k, _ in per), "pcg": sum(p for _, p in per),
-                     "pcg_per_newton_by_step": [round(p / max(k, 1), 1) for k, p in per],
-                     "newton_by_step": [k for k, _ in per]}
-    out["mixed_vs_fp64_rel_at_step"] = k64
-    out["mixed_vs_fp64_rel"] = float(torch.linalg.norm(runs["mixed_at_fp64_steps"] -
-                                                       runs["fp64"]) /
-                                     torch.linalg.norm(runs["fp64"]))
-    # adjoint of the top-face loss against u* from the log-normal field
+        return u, {"s": round(time.perf_counter() - t0, 2),
+                   "newton": sum(k for k, _ in per), "pcg": sum(p for _, p in per),
+                   "newton_by_step": [k for k, _ in per],
+                   "pcg_per_newton_by_step": [round(p / max(k, 1), 2) for k, p in per]}
+
+    u_m, out["mixed"] = path(L.FM_MIXED, "mixed")
+    u_d, out["fp64"] = path(L.FM_FP64, "fp64")
+    out["mixed_vs_fp64_rel"] = float(torch.linalg.norm(u_m - u_d) / torch.linalg.norm(u_d))
+    # u* from the 'true' field, then the adjoint of the top-face loss
     sel = torch.as_tensor(configs.top_face_xy_dofs(P.xyz), device="cuda")
-    Et = P.meta["E_true"]
-    ctx.set_material(P.E, nu, Et)
-    u_t, *_ = _solve_path(ctx, n, P.n_steps, L.FM_MIXED, a.inner_tol,
-                          line_search=a.line_search, max_newton=a.max_newton)
+    ctx.set_material(P.E, nu, P.meta["E_true"])
+    u_t, out["forward_true_mixed"] = path(L.FM_MIXED, "true")
     ctx.set_material(P.E, nu, P.E_elem)
-    u = runs["mixed"]
-    g = torch.zeros_like(u)
-    g[sel] = u[sel] - u_t[sel]
-    # FP64 arithmetic with a moderate inner tolerance (the outer defect
-    # correction sets the accuracy; a 1e-12 inner solve only costs time here)
-    gm64, _, _, s64, p64 = ctx.adjoint(u, g, tol=1e-11, inner_tol=1e-8, prec=L.FM_FP64)
-    gm32, _, _, s32, p32 = ctx.adjoint(u, g, tol=1e-11, inner_tol=0.1, prec=L.FM_MIXED)
-    out["adjoint"] = {"fp64_sweeps": s64, "fp64_pcg": p64, "mixed_sweeps": s32,
-                      "mixed_pcg": p32,
+    g = torch.zeros_like(u_d)
+    g[sel] = u_d[sel] - u_t[sel]
+    t0 = time.perf_counter()
+    gm64, _, _, s64, p64 = ctx.adjoint(u_d, g, tol=1e-10, inner_tol=1e-6, max_sweeps=a.sweeps,
+                                       prec=L.FM_FP64)
+    t64 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    gm32, _, _, s32, p32 = ctx.adjoint(u_d, g, tol=1e-10, inner_tol=0.1, max_sweeps=a.sweeps,
+                                       prec=L.FM_MIXED)
+    t32 = time.perf_counter() - t0
+    out["adjoint"] = {"fp64_sweeps": s64, "fp64_pcg": p64, "fp64_s": round(t64, 2),
+                      "mixed_sweeps": s32, "mixed_pcg": p32, "mixed_s": round(t32, 2),
+                      "loss": float(0.5 * torch.sum(g[sel] ** 2)),
                       "dLdmu_norm": float(torch.linalg.norm(gm64)),
                       "mixed_vs_fp64_rel": float(torch.linalg.norm(gm32 - gm64) /
                                                  torch.linalg.norm(gm64))}
@@ -393,6 +397,7 @@ def main(argv=None):
     ap.add_argument("--ilu-every", type=int, default=1)
     ap.add_argument("--initial-guess", type=int, default=0)
     ap.add_argument("--save-u", default=None)
+    ap.add_argument("--sweeps", type=int, default=500)
     a = ap.parse_args(argv)
     if not torch.cuda.is_available():
         raise SystemExit("cases need a CUDA device")
