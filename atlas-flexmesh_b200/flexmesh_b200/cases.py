@@ -191,10 +191,11 @@ def _solve_path(ctx, n, n_steps, prec, inner_tol, rtol=1e-10, u0=None, steps=Non
 
 
 def case_newton(a):
-    """Load levels 1 .. a.levels of the scale-up block in mixed precision with
-    the benchmark's Newton settings (inner PCG to 0.2, predictor to 1e-6,
-    the engine's line search), timed and broken down by kernel class: a
-    small, self-contained command for launch lists."""
+    """Load levels 1 .. a.levels of the scale-up block in mixed precision
+    with the engine's line search and the given inner tolerance, predictor
+    tolerance, ILU(0) interval and initial-guess setting (bench.py's MIXED
+    dict holds the benchmark's), timed and broken down by kernel class: a
+    small, self-contained command for settings sweeps and launch lists."""
     P = configs.scaleup_block(a.N)
     ctx = problem_context(P)
     u = torch.zeros(P.xyz.size, dtype=torch.float64, device="cuda")
