@@ -228,6 +228,8 @@ struct NewtonSolverConfig {
     double inner_tol = 1e-12;         // PCG tolerance of each Newton correction
     int max_pcg = 5000;
     fm_precision precision = FM_FP64;
+    int ilu_every = 1;                // ILU(0) refactored every ilu_every solves
+    int initial_guess = 0;            // FM_MIXED: PCG from the projected previous correction
 };
 
 struct NewtonSolverResult {
@@ -260,6 +262,16 @@ struct has_precision : std::false_type {};
 template <class T>
 struct has_precision<T, std::void_t<decltype(std::declval<const T&>().precision)>>
     : std::true_type {};
+template <class T, class = void>
+struct has_ilu_every : std::false_type {};
+template <class T>
+struct has_ilu_every<T, std::void_t<decltype(std::declval<const T&>().ilu_every)>>
+    : std::true_type {};
+template <class T, class = void>
+struct has_initial_guess : std::false_type {};
+template <class T>
+struct has_initial_guess<T, std::void_t<decltype(std::declval<const T&>().initial_guess)>>
+    : std::true_type {};
 }  // namespace detail
 
 // NonlinearNewtonSolver with the engine's mathematics: element tangent and
@@ -273,7 +285,8 @@ struct has_precision<T, std::void_t<decltype(std::declval<const T&>().precision)
 // BoundaryConditions (.dirichlet_bcs), LoadStep (.load_factor) and
 // NewtonSolverConfig (max_iterations, tol_absolute, tol_relative,
 // max_line_search) pass unchanged; the B200 fields of this header's
-// NewtonSolverConfig (inner_tol, max_pcg, precision) are read where present.
+// NewtonSolverConfig (inner_tol, max_pcg, precision, ilu_every,
+// initial_guess) are read where present.
 template <class Mesh, class Material = NeoHookeanMaterial, class BCs = BoundaryConditions>
 class NonlinearNewtonSolver {
 public:
@@ -309,6 +322,9 @@ public:
         if constexpr (detail::has_inner_tol<Config>::value) g.inner_tol = config.inner_tol;
         if constexpr (detail::has_max_pcg<Config>::value) g.max_pcg = config.max_pcg;
         if constexpr (detail::has_precision<Config>::value) g.precision = config.precision;
+        if constexpr (detail::has_ilu_every<Config>::value) g.ilu_every = config.ilu_every;
+        if constexpr (detail::has_initial_guess<Config>::value)
+            g.initial_guess = config.initial_guess;
         fm_newton_result res;
         const fm_status s = fm_newton_step_cfg_host(ctx.get(), u.data(), load.load_factor, &g,
                                                     &res);
