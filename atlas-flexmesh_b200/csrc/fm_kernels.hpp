@@ -126,8 +126,9 @@ void launch_norm2(uint32_t n, const double* R, double* partials, unsigned* count
 // b32 = R * inv_scale (FP32), x32 = 0 (x32 nullable)
 void launch_to_f32_scaled(uint32_t n, const double* R, double inv_scale, float* b32, float* x32,
                           cudaStream_t s);
-// x *= g (FP32)
+// x *= g
 void launch_scale_f32(uint32_t n, float* x, float g, cudaStream_t s);
+void launch_scale_f64(uint32_t n, double* x, double g, cudaStream_t s);
 // u += du (FP64)
 void launch_axpy_u(uint32_t n, const double* du, double* u, cudaStream_t s);
 // u += scale * du32
