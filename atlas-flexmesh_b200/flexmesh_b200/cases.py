@@ -328,7 +328,8 @@ def case_incompressible(a):
     ctx = problem_context(P)
     n = ctx.n_dofs
     out = {"case": "incompressible", "N": a.N, "tets": ctx.n_elems, "nu": nu,
-           "load_steps": P.n_steps, "inner_tol": a.inner_tol, "ilu_every": a.ilu_every}
+           "load_steps": min(a.steps, P.n_steps), "of": P.n_steps, "inner_tol": a.inner_tol,
+           "ilu_every": a.ilu_every}
     base = dict(newton_rtol=1e-10, inner_tol=a.inner_tol, predictor_tol=1e-6,
                 max_newton=a.max_newton, max_pcg=20000, line_search=10, ls_c=1e-4,
                 ilu_every=a.ilu_every)
@@ -339,7 +340,7 @@ def case_incompressible(a):
         t0 = time.perf_counter()
         u = torch.zeros(n, dtype=torch.float64, device="cuda")
         per = []
-        for s in range(1, P.n_steps + 1):
+        for s in range(1, min(a.steps, P.n_steps) + 1):
             r = ctx.newton_step_cfg(u, s / P.n_steps, **cfg)
             per.append((r["newton_iters"], r["pcg_iters"]))
             print(f"[{label}] step {s}: newton {per[-1][0]} pcg {per[-1][1]} "
@@ -399,6 +400,7 @@ def main(argv=None):
     ap.add_argument("--initial-guess", type=int, default=0)
     ap.add_argument("--save-u", default=None)
     ap.add_argument("--sweeps", type=int, default=500)
+    ap.add_argument("--steps", type=int, default=1000, help="load steps to run (all by default)")
     a = ap.parse_args(argv)
     if not torch.cuda.is_available():
         raise SystemExit("cases need a CUDA device")
