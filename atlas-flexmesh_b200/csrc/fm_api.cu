@@ -1297,9 +1297,7 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
     // ILU(0) of the eliminated tangent, PCG on R (norm rnorm) to itol, then
     // either u += du or du kept in `du` (FP64) for the line search.
     int n_solve = 0;
-    // the previous Newton correction is at hand (w32.x per ||R|| in mixed
-    // precision, du in FP64)
-    bool have_prev = false;
+    bool have_prev = false;  // w32.x holds the previous Newton correction / ||R||
     auto solve = [&](double rnorm, double itol, bool keep, int* its, bool newton) -> fm_status {
         const bool refactor = n_solve++ % g->ilu_every == 0;
         if (mixed) {
@@ -1340,34 +1338,11 @@ fm_status fm_newton_step_cfg(fm_ctx* c, double* u, double load_frac, const fm_ne
             have_prev = newton;
         } else {
             if (refactor) TRY(ilu_core<double>(c, c->fem, c->w64.K.p, c->w64.LU.p, c->w64.diag.p));
-            if (g->initial_guess && newton && have_prev) {
-                // du still holds the previous correction: start from its
-                // energy-norm projection, as the mixed path does
-                {
-                    PROF(FM_PROF_SPMV, 1);
-                    fm::launch_spmv_nodes<double>(c->nn, c->nbr_ptr.p, c->nbr.p, c->w64.K.p, du,
-                                                  c->w64.Ap.p, nullptr, nullptr, nullptr,
-                                                  c->stream);
-                }
-                {
-                    PROF(FM_PROF_VECTOR, 2);
-                    fm::launch_dot<double>(c->n, du, R, c->partials.p, c->counter(),
-                                           &c->sc.p->guess_xb, c->stream);
-                    fm::launch_dot<double>(c->n, du, c->w64.Ap.p, c->partials.p, c->counter(),
-                                           &c->sc.p->guess_xkx, c->stream);
-                }
-                TRY(sync_scalars(c));
-                const double xkx = c->h_sc->guess_xkx;
-                const double gam = xkx > 0.0 && std::isfinite(xkx) ? c->h_sc->guess_xb / xkx : 0.0;
-                { PROF(FM_PROF_VECTOR, 1); fm::launch_scale_f64(c->n, du, gam, c->stream); }
-            } else {
-                CK(cudaMemsetAsync(du, 0, sizeof(double) * c->n, c->stream));
-            }
+            CK(cudaMemsetAsync(du, 0, sizeof(double) * c->n, c->stream));
             Op<double> A{c, &c->fem, true, c->w64.K.p, c->w64.LU.p, c->w64.diag.p, c->w64.t.p,
                          c->grid_trsv64, c->w64.dinv.p};
             TRY(pcg_core<double>(c, A, c->n, R, du, itol, g->max_pcg, its, nullptr));
             if (!keep) { PROF(FM_PROF_VECTOR, 1); fm::launch_axpy_u(c->n, du, u, c->stream); }
-            have_prev = newton;
         }
         CK(cudaGetLastError());
         return FM_OK;

@@ -863,9 +863,6 @@ __global__ void k_scale(uint32_t n, T* __restrict__ x, T g) {
 void launch_scale_f32(uint32_t n, float* x, float g, cudaStream_t s) {
     k_scale<float><<<kRedBlocks * 2, kVecThreads, 0, s>>>(n, x, g);
 }
-void launch_scale_f64(uint32_t n, double* x, double g, cudaStream_t s) {
-    k_scale<double><<<kRedBlocks * 2, kVecThreads, 0, s>>>(n, x, g);
-}
 void launch_to_f32_scaled(uint32_t n, const double* R, double inv_scale, float* b32, float* x32,
                           cudaStream_t s) {
     k_to_f32_scaled<<<kRedBlocks * 2, kVecThreads, 0, s>>>(n, R, inv_scale, b32, x32);

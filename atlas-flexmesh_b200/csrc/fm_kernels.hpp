@@ -128,7 +128,6 @@ void launch_to_f32_scaled(uint32_t n, const double* R, double inv_scale, float* 
                           cudaStream_t s);
 // x *= g
 void launch_scale_f32(uint32_t n, float* x, float g, cudaStream_t s);
-void launch_scale_f64(uint32_t n, double* x, double g, cudaStream_t s);
 // u += du (FP64)
 void launch_axpy_u(uint32_t n, const double* du, double* u, cudaStream_t s);
 // u += scale * du32

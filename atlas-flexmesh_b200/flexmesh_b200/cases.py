@@ -314,9 +314,9 @@ def case_adjoint(a):
 def case_incompressible(a):
     """Near-incompressible block (48^3 x 6 tets, jitter 0.1 h, nu = 0.49,
     u_z = -0.4 in 20 load steps), the whole load path in mixed precision and
-    in FP64 with the same inexact-Newton settings (inner PCG to a.inner_tol
-    from the projected previous correction, ILU(0) every a.ilu_every solves,
-    the engine's line search), Newton and PCG
+    in FP64 with the same inexact-Newton settings (inner PCG to a.inner_tol,
+    mixed from the projected previous correction, ILU(0) every a.ilu_every
+    solves, the engine's line search), Newton and PCG
     counts per load step, the mixed-vs-FP64 difference at the end, and the
     adjoint dL/dmu (FP64 and mixed) for L = 1/2 |u_top - u*|^2 with u* from
     the log-normal mu field (sigma 0.2).  The reference's tangent clamps its
@@ -335,7 +335,7 @@ def case_incompressible(a):
                 ilu_every=a.ilu_every)
 
     def path(prec, label):
-        cfg = dict(base, prec=prec, initial_guess=1)
+        cfg = dict(base, prec=prec, initial_guess=1 if prec == L.FM_MIXED else 0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         u = torch.zeros(n, dtype=torch.float64, device="cuda")

@@ -338,10 +338,13 @@ typedef struct {
                               solve of a load step (1: every solve, as pcg_solve_ilu0
                               does; k > 1: an earlier tangent's factors precondition
                               the current tangent, which PCG still solves) */
-    int initial_guess;     /* 1 starts each Newton correction's PCG from gamma x_prev, the
-                              previous correction scaled by the energy-norm projection
-                              gamma = x_prev.b / x_prev.K x_prev; 0 starts from zero as
-                              pcg_solve_ilu0's callers do (the FP64 parity path) */
+    int initial_guess;     /* mixed precision: 1 starts each Newton correction's PCG from
+                              gamma x_prev, the previous correction (per ||R||) scaled by
+                              the energy-norm projection gamma = x_prev.b / x_prev.K x_prev;
+                              0 starts from zero as pcg_solve_ilu0's callers do.  FP64
+                              ignores it: its PCG keeps the reference's absolute early
+                              exit (||b - A x0|| < tol 1e-3) on the unscaled R, which a
+                              good x0 would trigger before any iteration */
 } fm_newton_config;
 
 typedef struct {

@@ -104,20 +104,6 @@ def test_scaleup16_path_mixed_bench_settings_within_1e8(fm, path16):
     assert rel(u.cpu().numpy(), path16["u_level10"]) <= TOL_MIXED
 
 
-def test_scaleup16_fp64_projected_guess_reaches_oracle_state(fm, path16):
-    """FP64 with the projected initial guess and a loose inner tolerance
-    (an option; the parity path starts every PCG from zero): the same
-    converged state after load level 5 as the oracle's tight solves"""
-    ctx, P = scaleup_ctx(fm)
-    u = torch.zeros(P.xyz.size, dtype=torch.float64, device="cuda")
-    for s in range(1, 6):
-        r = ctx.newton_step_cfg(u, s / P.n_steps, newton_rtol=1e-10, inner_tol=0.3,
-                                predictor_tol=1e-6, max_newton=400, max_pcg=20000,
-                                line_search=10, ls_c=1e-4, initial_guess=1, prec=fm.FM_FP64)
-        assert r["status"] == 0
-    assert rel(u.cpu().numpy(), path16["u_level5"]) <= TOL_MIXED
-
-
 def one_step_case(N=4, uz=-0.5):
     from flexmesh_b200 import configs
 
