@@ -47,7 +47,7 @@ WORKLOAD = "scale-up block 64^3x6 tets (1,572,864 tets, 823,875 DOF), jitter 0.1
 # c = 1e-4, FEM/adaptive_fem_engine.hpp:2581): without it the reference's
 # tangent stops contracting at load levels 8-10 of this block.  Mixed: inner
 # PCG to 0.8 from the projected previous correction, ILU(0) refactored every
-# third solve (the fastest of the measured settings; at most 156 Newton
+# third solve (the fastest of the measured settings; at most 145 Newton
 # iterations in a load step against the cap of 400, where 0.9 needs more
 # than 400 at load level 6; every Newton stop test is on the FP64 residual,
 # so all converge to the same u).
