@@ -36,11 +36,14 @@
 // (lanes without a neighbour add zeros), so both paths give the same values.
 //
 // Measured on B200 at 64^3 x 6 tets, FP32 (per forward+backward pair):
-// 0.716 ms grid-wide, 0.492 ms here with 24 warps per CTA (FP64: 0.806 ->
-// 0.710 ms with 16).  A per-node %globaltimer trace put the in-cluster hop
-// at 128 ns median against 480 ns through L2, and showed a build with one
-// node per warp bound by the warps' own per-node work (0.83 us issuing the
-// next node's loads); two nodes per warp halved that work per node.
+// 0.716 ms grid-wide, 0.467 ms here with 24 warps per CTA (FP64: 0.806 ->
+// 0.691 ms with 16).  A per-node %globaltimer trace of the critical path
+// (384 nodes per direction) splits a level into the hop (last dependency
+// pushed -> the reader's wait ends, ~300 ns, set by the poll round: ~150 ns
+// per round when the warp polls shared memory only, ~500 ns when a lane
+// polls L2) and the node's own work (wait end -> push, ~260 ns: products,
+// four butterfly rounds, finish, stores).  Two nodes per warp halved the
+// per-node work of a one-node-per-warp build.
 //
 // The backward solve runs its slabs in reverse block order (the top slab on
 // the first clusters), so in both directions clusters only wait on clusters
@@ -129,10 +132,32 @@ __device__ __forceinline__ void push_pre(const PushSolve& P, const NodeSched& S,
 // Bounded lock-step wait for the lane's neighbour's three values, from this
 // CTA's shared memory (sl) or from global memory (gp; neither: no
 // neighbour).  On a timeout FM_FLAG_TIMEOUT is set and the values may
-// still be sentinels.
+// still be sentinels.  When no lane of the warp reads global memory (three
+// warp steps in four at 64^3), every lane runs the same branch-free loop of
+// shared-memory polls, lanes without a neighbour on zero, a slot that
+// always holds zeros: the per-lane branches of the general loop doubled the
+// time of a poll round (about 150 against 320 ns in a %globaltimer trace).
 template <typename T>
-__device__ __forceinline__ void wait_push(uint32_t sl, const T* gp, unsigned* status,
-                                          unsigned m, T& v0, T& v1, T& v2) {
+__device__ __forceinline__ void wait_push(uint32_t sl, const T* gp, uint32_t zero,
+                                          unsigned* status, unsigned m, T& v0, T& v1, T& v2) {
+    if (!__any_sync(m, gp != nullptr)) {
+        const uint32_t a = sl != ~0u ? sl : zero;
+        ld_slot_cta(a, v0, v1, v2);
+        bool need = Sentinel<T>::is(v0) | Sentinel<T>::is(v1) | Sentinel<T>::is(v2);
+        if (!__any_sync(m, need)) return;
+        const long long t0 = clock64(), limit = wait_limit(status);
+        for (unsigned it = 1;; ++it) {
+            ld_slot_cta(a, v0, v1, v2);
+            need = Sentinel<T>::is(v0) | Sentinel<T>::is(v1) | Sentinel<T>::is(v2);
+            if (!__any_sync(m, need)) return;
+            if ((it & 255u) == 0 &&
+                __any_sync(m, (ld_volatile_u32(status) & FM_FLAG_TIMEOUT) ||
+                                  clock64() - t0 > limit)) {
+                if ((threadIdx.x & 15) == 0) raise_flag(status, FM_FLAG_TIMEOUT);
+                return;
+            }
+        }
+    }
     v0 = v1 = v2 = T(0);
     auto poll = [&]() {
         if (sl != ~0u) {
@@ -170,21 +195,28 @@ __device__ __forceinline__ void wait_push(uint32_t sl, const T* gp, unsigned* st
 // runs only over the lanes that can hold neighbours (8 or 16, the same for
 // the whole warp); the other lanes hold zeros, so the sums are those of a
 // full butterfly.  Lanes hl < kPushMax of each half hold its results.
+// zero: a slot of this CTA that always holds zeros.
 template <typename T, bool Lower>
-__device__ __forceinline__ void push_node(const PushPre<T>& Q, uint32_t base, T* out,
-                                          unsigned* status, int hl, unsigned m) {
+__device__ __forceinline__ void push_node(const PushPre<T>& Q, uint32_t base, uint32_t zero,
+                                          T* out, unsigned* status, int hl, unsigned m) {
     const bool has = hl < Q.cnt;
     const bool local = has && Q.sv != ~0u;
+    // resolved before the wait, off the chain: the reading CTA's slot address
+    // and the butterfly's width
+    const uint32_t pa =
+        Q.pe != ~0u ? mapa(base + (Q.pe & 0xfffffu) * kSlotBytes<T>, Q.pe >> 20) : 0u;
+    const bool wide = __any_sync(m, Q.cnt > 8);
     T v0, v1, v2;
     wait_push<T>(local ? base + Q.sv * kSlotBytes<T> : ~0u,
-                 has && !local ? out + 3 * (size_t)Q.nb : nullptr, status, m, v0, v1, v2);
+                 has && !local ? out + 3 * (size_t)Q.nb : nullptr, zero, status, m, v0, v1,
+                 v2);
     T s0 = T(0), s1 = T(0), s2 = T(0);
     if (has) {
         s0 = Q.a[0] * v0 + Q.a[1] * v1 + Q.a[2] * v2;
         s1 = Q.a[3] * v0 + Q.a[4] * v1 + Q.a[5] * v2;
         s2 = Q.a[6] * v0 + Q.a[7] * v1 + Q.a[8] * v2;
     }
-    if (__any_sync(m, Q.cnt > 8)) {
+    if (wide) {
         s0 += __shfl_xor_sync(m, s0, 8);
         s1 += __shfl_xor_sync(m, s1, 8);
         s2 += __shfl_xor_sync(m, s2, 8);
@@ -206,8 +238,7 @@ __device__ __forceinline__ void push_node(const PushPre<T>& Q, uint32_t base, T*
         x1 = (Q.c[1] - s1 - Q.c[5] * x2) * Q.s[1];
         x0 = (Q.c[0] - s0 - Q.c[3] * x1 - Q.c[4] * x2) * Q.s[0];
     }
-    if (Q.pe != ~0u)
-        st_slot_cluster(mapa(base + (Q.pe & 0xfffffu) * kSlotBytes<T>, Q.pe >> 20), x0, x1, x2);
+    if (Q.pe != ~0u) st_slot_cluster(pa, x0, x1, x2);
     if (hl == 0) {
         T* o = out + 3 * (size_t)Q.n;
         st_relaxed(o, x0);
@@ -230,7 +261,9 @@ __global__ void __launch_bounds__(push_max_warps(sizeof(T)) * 32, 1)
                 const T* __restrict__ rhs, T* __restrict__ out, T* __restrict__ fill,
                 uint32_t n_fill, unsigned* __restrict__ status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(16) T zero_slot[4];
     T* slots = reinterpret_cast<T*>(smem_raw);
+    if (threadIdx.x < 4) zero_slot[threadIdx.x] = T(0);
     const uint32_t cs = P.cluster, n_cl = P.n_ctas / cs;
     const uint32_t cl = blockIdx.x / cs, rank = blockIdx.x % cs;
     const uint32_t g = (Lower ? cl : n_cl - 1 - cl) * cs + rank;
@@ -273,7 +306,7 @@ __global__ void __launch_bounds__(push_max_warps(sizeof(T)) * 32, 1)
             const bool more = q + 1 < nq;
             if (more)
                 push_pre<T, Lower>(P, S, q + 1 < mine, rec_of(q + 1, cb), lu, dinv, rhs, hl, nxt);
-            push_node<T, Lower>(cur, base, out, status, hl, m);
+            push_node<T, Lower>(cur, base, smem_u32(zero_slot), out, status, hl, m);
             ++q;
             if ((q & 15) == 0 && more) {
                 ba = bb;
