@@ -391,7 +391,7 @@ static std::vector<uint4> node_records(const fm::NodeGraph& g, const std::vector
 // plan first tries to fit FP64 slots, else FP32 only) and no node has more
 // than 16 neighbours on a side.  The default path; FM_TRSV_PATH=pipe selects
 // the grid-wide pipelined solves (fm_trsv.cu) instead.  FM_TRSV_PUSH_WARPS caps the warps per CTA
-// (default: 24 in FP32, 16 in FP64), FM_TRSV_PUSH_BLOCK sets the interleave
+// (default: 32 in FP32, 16 in FP64), FM_TRSV_PUSH_BLOCK sets the interleave
 // block (default: chosen by the plan).
 fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
                             const std::vector<uint32_t>& lo, const std::vector<uint32_t>& up,

@@ -57,7 +57,7 @@ struct PushSolve {
     const uint32_t* nslot_b = nullptr;
 };
 // most warps per CTA of the push kernels of this value width (register budget)
-constexpr int push_max_warps(size_t value_bytes) { return value_bytes == 4 ? 24 : 16; }
+constexpr int push_max_warps(size_t value_bytes) { return value_bytes == 4 ? 32 : 16; }
 // dynamic shared memory of one CTA of a direction with max_slot slots
 size_t push_smem_bytes(uint32_t max_slot, size_t value_bytes);
 // clusters of `cluster` CTAs (warps each, smem bytes) that can be resident

@@ -36,7 +36,7 @@
 // (lanes without a neighbour add zeros), so both paths give the same values.
 //
 // Measured on B200 at 64^3 x 6 tets, FP32 (per forward+backward pair):
-// 0.716 ms grid-wide, 0.467 ms here with 24 warps per CTA (FP64: 0.806 ->
+// 0.716 ms grid-wide, 0.444 ms here with 32 warps per CTA (FP64: 0.806 ->
 // 0.691 ms with 16).  A per-node %globaltimer trace of the critical path
 // (384 nodes per direction) splits a level into the hop (last dependency
 // pushed -> the reader's wait ends, ~300 ns, set by the poll round: ~150 ns
@@ -296,27 +296,47 @@ __global__ void __launch_bounds__(push_max_warps(sizeof(T)) * 32, 1)
         auto rec_of = [&](uint32_t q, uint32_t cb) {
             return shfl4((q >> 4) == cb ? ba : bb, (lane & 16) | (int)(q & 15), m);
         };
-        PushPre<T> qa, qb;
-        push_pre<T, Lower>(P, S, 0 < mine, rec_of(0, 0), lu, dinv, rhs, hl, qa);
-        uint32_t q = 0;
-        // cur is processed while nxt's loads are in flight; the two swap
-        // roles every step (no register copies that would wait on them)
-        auto step = [&](const PushPre<T>& cur, PushPre<T>& nxt) {
-            const uint32_t cb = q >> 4;
-            const bool more = q + 1 < nq;
-            if (more)
-                push_pre<T, Lower>(P, S, q + 1 < mine, rec_of(q + 1, cb), lu, dinv, rhs, hl, nxt);
-            push_node<T, Lower>(cur, base, smem_u32(zero_slot), out, status, hl, m);
-            ++q;
-            if ((q & 15) == 0 && more) {
-                ba = bb;
-                bb = batch((q >> 4) + 1);
+        if constexpr (sizeof(T) == 4) {
+            // FP32: one node's loads at a time, issued when the warp reaches
+            // the node (a warp's consecutive nodes are mostly several levels
+            // apart); the registers this frees give 32 warps per CTA instead
+            // of 24 (0.444 against 0.467 ms per pair at 64^3)
+            for (uint32_t q = 0; q < nq; ++q) {
+                PushPre<T> qa;
+                push_pre<T, Lower>(P, S, q < mine, rec_of(q, q >> 4), lu, dinv, rhs, hl, qa);
+                push_node<T, Lower>(qa, base, smem_u32(zero_slot), out, status, hl, m);
+                if (((q + 1) & 15) == 0 && q + 1 < nq) {
+                    ba = bb;
+                    bb = batch(((q + 1) >> 4) + 1);
+                }
             }
-            return more;
-        };
-        for (;;) {
-            if (!step(qa, qb)) break;
-            if (!step(qb, qa)) break;
+        } else {
+            // FP64: the next node's loads in flight while the warp waits on
+            // the current one (single-buffered at 20 or 24 warps it was
+            // slower than this at 16)
+            PushPre<T> qa, qb;
+            push_pre<T, Lower>(P, S, 0 < mine, rec_of(0, 0), lu, dinv, rhs, hl, qa);
+            uint32_t q = 0;
+            // cur is processed while nxt's loads are in flight; the two swap
+            // roles every step (no register copies that would wait on them)
+            auto step = [&](const PushPre<T>& cur, PushPre<T>& nxt) {
+                const uint32_t cb = q >> 4;
+                const bool more = q + 1 < nq;
+                if (more)
+                    push_pre<T, Lower>(P, S, q + 1 < mine, rec_of(q + 1, cb), lu, dinv, rhs, hl,
+                                       nxt);
+                push_node<T, Lower>(cur, base, smem_u32(zero_slot), out, status, hl, m);
+                ++q;
+                if ((q & 15) == 0 && more) {
+                    ba = bb;
+                    bb = batch((q >> 4) + 1);
+                }
+                return more;
+            };
+            for (;;) {
+                if (!step(qa, qb)) break;
+                if (!step(qb, qa)) break;
+            }
         }
     }
     if (n_fill) {
