@@ -386,20 +386,23 @@ static std::vector<uint4> node_records(const fm::NodeGraph& g, const std::vector
 }
 
 // Plan of the slab-partitioned push solves (fm_trsv_push.cu): one slab per
-// cluster of 8 CTAs, as many clusters as the device keeps resident (FP32 and
-// FP64 kernels alike), when every CTA's slots fit its shared memory (the
+// thread-block cluster, as many clusters as the device keeps resident (FP32
+// and FP64 kernels alike), when every CTA's slots fit its shared memory (the
 // plan first tries to fit FP64 slots, else FP32 only) and no node has more
-// than 16 neighbours on a side.  The default path; FM_TRSV_PATH=pipe selects
-// the grid-wide pipelined solves (fm_trsv.cu) instead.  FM_TRSV_PUSH_WARPS caps the warps per CTA
-// (default: 32 in FP32, 16 in FP64), FM_TRSV_PUSH_BLOCK sets the interleave
-// block (default: chosen by the plan).
+// than 16 neighbours on a side.  The cluster size (8 or 9 CTAs) is the one
+// that keeps the most CTAs resident: a cluster must fit in one GPC, and on
+// B200 15 clusters of 9 (135 CTAs) are resident against 15 of 8 (measured
+// 0.436 against 0.450 ms per FP32 pair, 0.616 against 0.708 FP64, at 64^3).
+// The default path; FM_TRSV_PATH=pipe selects the grid-wide pipelined solves
+// (fm_trsv.cu) instead.  FM_TRSV_PUSH_WARPS caps the warps per CTA (default:
+// 32 in FP32, 16 in FP64), FM_TRSV_PUSH_BLOCK sets the interleave block
+// (default: chosen by the plan), FM_TRSV_PUSH_CLUSTER the cluster size.
 fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
                             const std::vector<uint32_t>& lo, const std::vector<uint32_t>& up,
                             const std::vector<uint32_t>& uo) {
     c->pu_ok32 = c->pu_ok64 = false;
     const char* path = getenv("FM_TRSV_PATH");
     if (path && std::strcmp(path, "push") != 0) return FM_OK;
-    constexpr uint32_t kCluster = 8;
     // dynamic shared memory per CTA at most; the kernels' static shared
     // memory (under 1 KB) takes the rest of the 227 KB
     constexpr size_t kMaxSmem = 226 * 1024;
@@ -410,16 +413,28 @@ fm_status setup_push_solves(fm_ctx* c, const std::vector<uint32_t>& lp,
     const int warps32 = env("FM_TRSV_PUSH_WARPS", fm::push_max_warps(4), 1, fm::push_max_warps(4));
     const int warps64 = std::min(warps32, fm::push_max_warps(8));
     const uint32_t block = (uint32_t)env("FM_TRSV_PUSH_BLOCK", 0, 0, 1 << 20);
-    const int nc32 = fm::push_max_clusters(4, kCluster, warps32, kMaxSmem);
-    const int nc64 = fm::push_max_clusters(8, kCluster, warps64, kMaxSmem);
-    const int ncl = std::min(nc32, nc64);
-    if (ncl < 1) return FM_OK;
+    // candidate cluster sizes, most resident CTAs first
+    std::vector<std::pair<int, uint32_t>> sizes;  // (resident clusters, size)
+    const int forced = env("FM_TRSV_PUSH_CLUSTER", 0, 0, (int)fm::kPushMax);
+    for (uint32_t cs = 8; cs <= fm::kPushMax; ++cs) {
+        if (forced && cs != (uint32_t)forced) continue;
+        const int ncl = std::min(fm::push_max_clusters(4, (int)cs, warps32, kMaxSmem),
+                                 fm::push_max_clusters(8, (int)cs, warps64, kMaxSmem));
+        if (ncl > 0) sizes.push_back({ncl, cs});
+    }
+    std::stable_sort(sizes.begin(), sizes.end(), [](const auto& a, const auto& b) {
+        return a.first * a.second > b.first * b.second;
+    });
     fm::PushPlan p;
-    if (!fm::push_plan(c->graph, lp, lo, up, uo, (uint32_t)ncl, kCluster, block,
-                       (uint32_t)(kMaxSmem / fm::push_smem_bytes(1, 8)), p) &&
-        !fm::push_plan(c->graph, lp, lo, up, uo, (uint32_t)ncl, kCluster, block,
-                       (uint32_t)(kMaxSmem / fm::push_smem_bytes(1, 4)), p))
-        return FM_OK;
+    bool planned = false;
+    for (const auto& sz : sizes) {
+        planned = fm::push_plan(c->graph, lp, lo, up, uo, (uint32_t)sz.first, sz.second, block,
+                                (uint32_t)(kMaxSmem / fm::push_smem_bytes(1, 8)), p) ||
+                  fm::push_plan(c->graph, lp, lo, up, uo, (uint32_t)sz.first, sz.second, block,
+                                (uint32_t)(kMaxSmem / fm::push_smem_bytes(1, 4)), p);
+        if (planned) break;
+    }
+    if (!planned) return FM_OK;
     auto fits = [&](size_t vb) {
         return fm::push_smem_bytes(std::max(p.max_slot_f, p.max_slot_b), vb) <= kMaxSmem;
     };

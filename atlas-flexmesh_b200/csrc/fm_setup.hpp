@@ -83,7 +83,7 @@ void ilu_edge_maps(const NodeGraph& g, std::vector<uint32_t>& ptr, std::vector<u
 // nodes are dealt round-robin to the cluster's CTAs, so that every CTA holds
 // a share of each level (block is chosen to keep the busiest CTA's share of
 // any level small).
-constexpr uint32_t kPushMax = 8;  // reading CTAs per producer, at most (= cluster size)
+constexpr uint32_t kPushMax = 9;  // reading CTAs per producer, at most (>= cluster size)
 struct PushPlan {
     uint32_t n_ctas = 0, cluster = 0, block = 0;
     uint32_t max_level_share = 0;  // most nodes of one level in one CTA

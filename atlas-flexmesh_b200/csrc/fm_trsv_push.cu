@@ -353,6 +353,10 @@ static void allow_smem(K kernel, size_t smem) {
     if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         cudaGetLastError();
+    // clusters of 9 CTAs are above the portable size of 8
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+        cudaSuccess)
+        cudaGetLastError();
 }
 
 template <typename K>
