@@ -6,7 +6,7 @@
 // N^3 block); in the grid-wide solves (fm_trsv.cu) every hop of the chain
 // is a value stored to L2 and polled back by another SM, ~0.43 us of the
 // ~0.92 us a level costs.  Here the node range is cut into one contiguous
-// slab per cluster (8 CTAs, one per SM), whose blocks of consecutive nodes
+// slab per cluster (9 CTAs on B200, one per SM), whose blocks of consecutive nodes
 // are dealt round-robin to the cluster's CTAs (so that each CTA holds a
 // share of every level).  The forward solve only waits on lower-numbered
 // nodes and the backward on higher-numbered ones, so any dependency chain
