@@ -575,10 +575,10 @@ fm_status pcg_core(fm_ctx* c, const Op<T>& A, uint32_t n, const T* b, T* x, doub
 
 template <typename T>
 fm_status ilu_core(fm_ctx* c, SolverCsr& S, const T* a, T* lu, T* diag) {
-    PROF(FM_PROF_ILU, 1);
+    PROF(FM_PROF_ILU, &S == &c->fem ? 3 : 1);
     if (&S == &c->fem) {
-        fm::launch_ilu0_nodes<T>(node_sched(c), a, lu, diag, work<T>(c).dinv.p, c->done.p,
-                                 next_epoch(c), c->status(), c->device, c->stream);
+        fm::launch_ilu0_nodes<T>(node_sched(c), a, lu, c->nnz, diag, work<T>(c).dinv.p,
+                                 c->status(), c->device, c->stream);
         CK(cudaGetLastError());
         return FM_OK;
     }

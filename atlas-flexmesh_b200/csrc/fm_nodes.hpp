@@ -31,10 +31,12 @@ struct NodeSched {
 template <typename T>
 void launch_trsv_nodes(const NodeSched& S, const T* lu, const T* dinv, const T* r, T* tmp, T* y,
                        unsigned* status, int device, cudaStream_t s);
-// LU (a_ii kept on diagonal slots), pivots d and their reciprocals dinv
+// LU (nnz entries, a_ii kept on diagonal slots), pivots d and their
+// reciprocals dinv (three kernels: LU and dinv filled with the wait
+// sentinel, then the factorization)
 template <typename T>
-void launch_ilu0_nodes(const NodeSched& S, const T* a, T* lu, T* d, T* dinv, unsigned* done,
-                       unsigned epoch, unsigned* status, int device, cudaStream_t s);
+void launch_ilu0_nodes(const NodeSched& S, const T* a, T* lu, uint64_t nnz, T* d, T* dinv,
+                       unsigned* status, int device, cudaStream_t s);
 template <typename T>
 void launch_fill_sentinel(uint32_t n, T* x, cudaStream_t s);
 
