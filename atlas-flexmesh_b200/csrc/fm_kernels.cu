@@ -292,11 +292,11 @@ __device__ __forceinline__ void asm_node(const MeshDev& m, const ElemRec<KT>* __
     }
 }
 
-// Four CTAs per SM: the FP64 pass fits 64 registers without spilling, and
-// 32 resident warps instead of 24 took it from 0.784 to 0.733 ms at 64^3
-// (the FP32 pass needs 48).
+// CTAs per SM: the FP64 pass fits 64 registers for four without spilling
+// (32 resident warps instead of 24: 0.784 -> 0.733 ms at 64^3), the FP32
+// pass 40 for six (0.540 -> 0.531 ms).
 template <typename KT>
-__global__ void __launch_bounds__(kAsmWarps * 32, 4)
+__global__ void __launch_bounds__(kAsmWarps * 32, sizeof(KT) == 4 ? 6 : 4)
     k_assemble(MeshDev m, const ElemRec<KT>* __restrict__ rec, KT* __restrict__ K,
                double* __restrict__ f, double* __restrict__ R, int apply_bc,
                unsigned* __restrict__ status) {
